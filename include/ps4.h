@@ -1,0 +1,162 @@
+/*
+ * ps4.h -- C-ABI of libps4.so, the B200 (sm_100a) search for sets of positive integers
+ * whose pairwise sums are all perfect squares.
+ *
+ * The reference exposes this path as a process (exhaustive/s4.c), not a library: its
+ * in-process seam is process_chunk(S0,S1,&work,&stats) (exhaustive/s4.c:280) feeding
+ * handle_4set (exhaustive/s4.c:225).  Each entry point below names the reference code it
+ * replaces.  Plain pointers and sizes only; every function returns 0 or a PS4_ERR_* code,
+ * with the message in ps4_last_error().  One host thread per context.
+ *
+ * Output records are raw (numbers, not text); ps4_format_* turn them into the reference's
+ * exact result lines (exhaustive/s4.c:24-27,110-137,209-220,237-277).
+ */
+#ifndef PS4_H
+#define PS4_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PS4_ABI_VERSION 1
+
+/* ---- status codes ---- */
+enum {
+    PS4_OK = 0,
+    PS4_ERR_ARG = 1,          /* bad argument (message says which)                                  */
+    PS4_ERR_CUDA = 3,         /* CUDA runtime failure, or no usable sm_100 device                   */
+    PS4_ERR_CAP_REPS = 10,    /* "representation capacity exceeded"  (s4.c:321)                    */
+    PS4_ERR_CAP_DIVS = 11,    /* "divisor capacity exceeded"         (s4.c:176)                    */
+    PS4_ERR_CAP_EXT = 12,     /* "extension capacity exceeded"       (s4.c:201)                    */
+    PS4_ERR_VERIFY = 13,      /* "quadruple verification failed"     (s4.c:232, --verify only)     */
+    PS4_ERR_OUTPUT_FULL = 20, /* a caller buffer in ps4_results is too small; n_* hold the needed sizes */
+    PS4_ERR_TIMEOUT = 21      /* a device-side bounded wait gave up (persistent kernels, serving)   */
+};
+
+/* ---- flags (ps4_config.flags) ---- */
+enum {
+    PS4_F_NOEXT = 1,   /* count 4-sets only, no extension step            (s4 --noext, s4.c:242)  */
+    PS4_F_VERIFY = 2,  /* re-check the six roots of every 4-set on device (s4 --verify, s4.c:229) */
+    PS4_F_DUMP4 = 4    /* return every 4-set as a ps4_quad record         (s4 --dump4, s4.c:237)  */
+};
+
+/* ---- kernel choice (ps4_config.kernel) ---- */
+enum {
+    PS4_KERNEL_BATCHED = 0, /* persistent tile queue, cost-binned extension, compacted square tests */
+    PS4_KERNEL_PLAIN = 1    /* one CTA per tile, one thread per S, inline extension (baseline)       */
+};
+
+typedef struct ps4_ctx ps4_ctx;
+
+typedef struct {
+    int device;            /* CUDA device ordinal                                                   */
+    uint64_t s_hi_max;     /* largest S_hi to be searched; sizes the factor tables (<= 2^44)         */
+    uint32_t cap_reps;     /* representation cap per S        (S4_MAX_REPS, default 512,   s4.c:46)  */
+    uint32_t cap_divs;     /* divisor cap per difference      (S4_MAX_DIVS, default 16384, s4.c:52)  */
+    uint32_t cap_ext;      /* extension cap per 4-set         (S4_MAX_EXT,  default 64,    s4.c:49)  */
+    uint32_t flags;        /* PS4_F_*                                                               */
+    uint32_t kernel;       /* PS4_KERNEL_*                                                          */
+    uint32_t log2_tile;    /* S values per tile = 2^log2_tile (12..14); 0 = autotuned/default        */
+    uint32_t ctas_per_sm;  /* resident CTAs per SM for the persistent kernel; 0 = default            */
+    void *stream;          /* cudaStream_t to launch on; NULL = a stream owned by the context        */
+} ps4_config;
+
+/* Counters, identical in meaning to the reference's stats_t (exhaustive/s4.c:80-91). */
+typedef struct {
+    uint64_t S_done, pairs, S_ge3, triples, sets4, sets5, sets6, multi, ext_cand, ext_sqrt;
+    uint64_t hist5[100];
+    uint64_t max_reps, max_divisors, max_extensions;
+} ps4_stats;
+
+/* A 4-set with at least one extension (what handle_4set prints about, s4.c:243-277). */
+typedef struct {
+    uint64_t S;
+    uint64_t v[4];        /* a,b,c,d in the reference's formula order (s4.c:333)                      */
+    uint32_t n_ext;       /* extensions, stored at exts[first_ext .. first_ext+n_ext) in the         */
+    uint32_t first_ext;   /*   reference's divisor order (s4.c:185-204)                              */
+    uint32_t flags;       /* PS4_HIT_*                                                               */
+    uint32_t item;        /* index of the query (subrange or triple) this hit belongs to              */
+    uint32_t order[4];    /* sort key reproducing the reference's emission order: px, py, pz, class   */
+} ps4_hit;
+
+enum { PS4_HIT_MULTI = 1,        /* >= 2 extensions: an "M:" line                    */
+       PS4_HIT_DRILL_OK = 2 };   /* {v, ext0, ext1} passes verify_set (drill line)   */
+
+typedef struct {
+    uint64_t lo, hi;      /* the extension e = hi*2^64 + lo                                          */
+    uint32_t key;         /* divisor index of the pair that produced e (reference order)             */
+    uint32_t flags;       /* PS4_EXT_*                                                               */
+} ps4_ext;
+
+enum { PS4_EXT_FIVE = 1,         /* e > max(v): a "5:" line                         */
+       PS4_EXT_FIVE_OK = 2 };    /* that 5-set passes verify_set                    */
+
+typedef struct {            /* a 6-set {v, ext t, ext s} (s4.c:270-276)                      */
+    uint32_t hit, t, s, flags;   /* flags bit 0: passes verify_set                            */
+} ps4_six;
+
+typedef struct {            /* one 4-set for --dump4: the six pair roots, formula order         */
+    uint32_t r_ab, r_ac, r_ad, r_bc, r_bd, r_cd;
+} ps4_quad;
+
+/* Caller-owned host output buffers.  On return n_* hold the record counts; if any
+ * count exceeds its *_cap the call returns PS4_ERR_OUTPUT_FULL, nothing is written
+ * past the caps, and the call can be repeated with larger buffers. */
+typedef struct {
+    ps4_hit *hits;   uint64_t hits_cap;   uint64_t n_hits;
+    ps4_ext *exts;   uint64_t exts_cap;   uint64_t n_exts;
+    ps4_six *sixes;  uint64_t sixes_cap;  uint64_t n_sixes;
+    ps4_quad *quads; uint64_t quads_cap;  uint64_t n_quads;
+} ps4_results;
+
+/* ---- lifetime ---- */
+
+/* Build the factor / divisor-count tables for S < cfg->s_hi_max on the device and
+ * allocate the working buffers.  (Replaces the table set-up of s4.c:436-447.) */
+int ps4_create(const ps4_config *cfg, ps4_ctx **out);
+void ps4_destroy(ps4_ctx *ctx);
+const char *ps4_last_error(const ps4_ctx *ctx);
+int ps4_abi_version(void);
+
+/* ---- the search ----
+ *
+ * Every S in [lo, hi): enumerate all 4-sets with sum S, extend each by divisor pairs,
+ * report every 4-set with >= 1 extension, and add the reference's counters into *stats
+ * (+=).  Replaces the worker loop over process_chunk (exhaustive/s4.c:344-364 calling
+ * :280-341, :225-278, :160-207).  Results are independent of how [lo,hi) is split into
+ * calls.  Host buffers; the call returns when results are in them. */
+int ps4_search_range(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res);
+
+/* Many independent subranges [lo[i], hi[i]) in ONE persistent launch (the block controller's
+ * sequence of s4 invocations, run_exhaustive.py:200-238, done as one device batch).  stats
+ * points at n_items ps4_stats (+=); every hit carries its item index.  Subranges may overlap;
+ * each is searched in full. */
+int ps4_search_batch(ps4_ctx *ctx, const uint64_t *lo, const uint64_t *hi, uint32_t n_items,
+                     ps4_stats *stats, ps4_results *res);
+
+/* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
+double ps4_last_kernel_ms(const ps4_ctx *ctx);
+/* Number of kernel launches made by the last search call. */
+uint64_t ps4_last_launches(const ps4_ctx *ctx);
+
+/* ---- text output, byte-identical to the reference ----
+ *
+ * Write the buffered result lines of `hit` -- the "M:" line, then the "5:" lines in
+ * extension order -- into buf, NUL-terminated (s4.c:247-269, format_set s4.c:214-220).
+ * Returns the length, or -1 if cap is too small.  `exts` is the results' ext array. */
+long ps4_format_hit(const ps4_hit *hit, const ps4_ext *exts, char *buf, size_t cap);
+/* The "!!!!!!!! FOUND 6-SET:" alert line of a 6-set record (s4.c:270-276).  Returns length or -1. */
+long ps4_format_six(const ps4_hit *hit, const ps4_ext *exts, const ps4_six *six, char *buf, size_t cap);
+/* The --test-sixset drill line for an M hit (s4.c:255-260).  Returns length or -1. */
+long ps4_format_drill(const ps4_hit *hit, const ps4_ext *exts, char *buf, size_t cap);
+/* A "4:" dump line (s4.c:239).  Returns length or -1. */
+long ps4_format_quad(const ps4_quad *q, char *buf, size_t cap);
+/* S, v[4] and the reference's emission-order key of a dump record. */
+void ps4_quad_values(const ps4_quad *q, uint64_t *S, uint64_t v[4], uint32_t order[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,350 @@
+// ps4_api.cu -- host side of the C-ABI (include/ps4.h): context, device tables, launches,
+// automatic re-runs on internal capacity limits, and result collection.
+//
+// Replaces the driver part of exhaustive/s4.c: table set-up (s4.c:436-447), the per-thread
+// chunk loop (s4.c:344-364) and the counter totals (s4.c:488-495).  One host thread per
+// context; every search call is synchronous on the context's stream.
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ps4_internal.h"
+
+using namespace ps4;
+
+struct ps4_ctx {
+    ps4_config cfg;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 0;
+    uint64_t tab_n = 0;
+    uint64_t *d_spfq = nullptr;
+    uint16_t *d_ndiv = nullptr;
+    // working buffers (grown on demand)
+    Item *d_items = nullptr; uint32_t items_cap = 0;
+    unsigned long long *d_counters = nullptr; uint32_t counters_items = 0;
+    ps4_hit *d_hits = nullptr; uint32_t hits_cap = 0;
+    ps4_ext *d_exts = nullptr; uint32_t exts_cap = 0;
+    ps4_six *d_sixes = nullptr; uint32_t sixes_cap = 0;
+    ps4_quad *d_quads = nullptr; uint64_t quads_cap = 0;
+    uint32_t *d_scratch = nullptr; size_t scratch_words = 0;
+    Status *d_status = nullptr;
+    Status *h_status = nullptr;          // pinned
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double last_ms = 0.0;
+    uint64_t last_launches = 0;
+    unsigned tile_log2 = 14;             // current tile size (may shrink on E_TILE)
+    std::string err;
+};
+
+static int set_err(ps4_ctx *c, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                          \
+    do {                                                                                             \
+        cudaError_t _e = (call);                                                                     \
+        if (_e != cudaSuccess)                                                                       \
+            return set_err(ctx, PS4_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e));      \
+    } while (0)
+
+template <class T>
+static int grow(ps4_ctx *c, T *&ptr, uint64_t &cap, uint64_t need) {
+    if (need <= cap && ptr) return 0;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    cap = 0;
+    if (need == 0) return 0;
+    CUDA_TRY(c, cudaMalloc((void **)&ptr, need * sizeof(T)));
+    cap = need;
+    return 0;
+}
+template <class T>
+static int grow32(ps4_ctx *c, T *&ptr, uint32_t &cap, uint64_t need) {
+    uint64_t cap64 = cap;
+    int rc = grow(c, ptr, cap64, need);
+    cap = (uint32_t)cap64;
+    return rc;
+}
+
+static uint64_t isqrt_host(uint64_t n) {
+    uint64_t r = (uint64_t)std::sqrt((double)n);
+    while (r * r > n) r--;
+    while ((r + 1) * (r + 1) <= n) r++;
+    return r;
+}
+
+extern "C" int ps4_abi_version(void) { return PS4_ABI_VERSION; }
+
+extern "C" const char *ps4_last_error(const ps4_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+extern "C" double ps4_last_kernel_ms(const ps4_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
+
+extern "C" uint64_t ps4_last_launches(const ps4_ctx *ctx) { return ctx ? ctx->last_launches : 0; }
+
+extern "C" void ps4_destroy(ps4_ctx *c) {
+    if (!c) return;
+    cudaFree(c->d_spfq); cudaFree(c->d_ndiv); cudaFree(c->d_items); cudaFree(c->d_counters);
+    cudaFree(c->d_hits); cudaFree(c->d_exts); cudaFree(c->d_sixes); cudaFree(c->d_quads);
+    cudaFree(c->d_scratch); cudaFree(c->d_status);
+    if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+static const uint64_t S_LIMIT = 1ull << 44;   // roots < 2^22: 4-set staging packs 10 bits above them
+
+extern "C" int ps4_create(const ps4_config *cfg, ps4_ctx **out) {
+    if (!cfg || !out) return PS4_ERR_ARG;
+    *out = nullptr;
+    ps4_ctx *c = new ps4_ctx();
+    c->cfg = *cfg;
+    if (c->cfg.cap_reps == 0) c->cfg.cap_reps = 512;
+    if (c->cfg.cap_divs == 0) c->cfg.cap_divs = 16384;
+    if (c->cfg.cap_ext == 0) c->cfg.cap_ext = 64;
+    if (c->cfg.s_hi_max < 2) c->cfg.s_hi_max = 2;
+    if (c->cfg.s_hi_max > S_LIMIT) {
+        int rc = set_err(c, PS4_ERR_ARG, "s_hi_max %llu exceeds the supported bound 2^44",
+                         (unsigned long long)c->cfg.s_hi_max);
+        *out = c;
+        return rc;
+    }
+    if (c->cfg.log2_tile) c->tile_log2 = std::min(14u, std::max(12u, c->cfg.log2_tile));
+    *out = c;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return set_err(c, PS4_ERR_CUDA, "no CUDA device available (libps4 has no CPU path)");
+    CUDA_TRY(c, cudaSetDevice(cfg->device));
+    cudaDeviceProp prop;
+    CUDA_TRY(c, cudaGetDeviceProperties(&prop, cfg->device));
+    if (prop.major != 10)
+        return set_err(c, PS4_ERR_CUDA, "device %d is sm_%d%d; libps4 is built for sm_100a only", cfg->device,
+                       prop.major, prop.minor);
+    c->num_sms = prop.multiProcessorCount;
+    if (cfg->stream) {
+        c->stream = (cudaStream_t)cfg->stream;
+    } else {
+        CUDA_TRY(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+        c->own_stream = true;
+    }
+    CUDA_TRY(c, cudaEventCreate(&c->ev0));
+    CUDA_TRY(c, cudaEventCreate(&c->ev1));
+    c->tab_n = 2 * isqrt_host(c->cfg.s_hi_max) + 64;      // s4.c:440
+    CUDA_TRY(c, cudaMalloc((void **)&c->d_spfq, c->tab_n * sizeof(uint64_t)));
+    CUDA_TRY(c, cudaMalloc((void **)&c->d_ndiv, c->tab_n * sizeof(uint16_t)));
+    CUDA_TRY(c, cudaMalloc((void **)&c->d_status, sizeof(Status)));
+    CUDA_TRY(c, cudaMallocHost((void **)&c->h_status, sizeof(Status)));
+    CUDA_TRY(c, (cudaError_t)launch_tables(c->d_spfq, c->d_ndiv, c->tab_n, c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    return PS4_OK;
+}
+
+static void stats_add(ps4_stats *s, const unsigned long long *k) {
+    uint64_t *add = &s->S_done;          // S_done .. ext_sqrt are contiguous
+    for (int i = 0; i < 10; i++) add[i] += k[i];
+    for (int i = 0; i < 100; i++) s->hist5[i] += k[K_HIST5 + i];
+    s->max_reps = std::max<uint64_t>(s->max_reps, k[K_MAX_REPS]);
+    s->max_divisors = std::max<uint64_t>(s->max_divisors, k[K_MAX_DIVS]);
+    s->max_extensions = std::max<uint64_t>(s->max_extensions, k[K_MAX_EXT]);
+}
+
+static const char *fatal_text(unsigned code) {
+    switch (code) {
+        case E_CAP_REPS: return "representation capacity exceeded";
+        case E_CAP_DIVS: return "divisor capacity exceeded";
+        case E_CAP_EXT: return "extension capacity exceeded";
+        case E_VERIFY: return "quadruple verification failed";
+        default: return "internal capacity exceeded";
+    }
+}
+
+// Run the search over n items (each [lo,hi)) in one launch, re-running on internal
+// capacity limits; results land in the device buffers.  stats: one per item (+=).
+static int run_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, ps4_stats *stats,
+                     ps4_results *res) {
+    std::vector<Item> items(n_items);
+    uint64_t tiles_total = 0;
+    c->last_launches = 0;
+    c->last_ms = 0.0;
+    for (uint32_t i = 0; i < n_items; i++) {
+        uint64_t a = std::max<uint64_t>(lo[i], 1), b = hi[i];
+        if (b > c->cfg.s_hi_max)
+            return set_err(c, PS4_ERR_ARG, "S_hi %llu exceeds the context's s_hi_max %llu", (unsigned long long)b,
+                           (unsigned long long)c->cfg.s_hi_max);
+        if (b < a) b = a;
+        items[i].lo = a;
+        items[i].hi = b;
+    }
+    if (grow32(c, c->d_items, c->items_cap, n_items)) return PS4_ERR_CUDA;
+    if (grow32(c, c->d_counters, c->counters_items, (uint64_t)n_items * K_SLOTS)) return PS4_ERR_CUDA;
+    const bool dump = (c->cfg.flags & PS4_F_DUMP4) && res && res->quads_cap > 0;
+    if (dump && grow(c, c->d_quads, c->quads_cap, res->quads_cap)) return PS4_ERR_CUDA;
+    if (grow32(c, c->d_hits, c->hits_cap, std::max<uint32_t>(c->hits_cap, 1u << 16))) return PS4_ERR_CUDA;
+    if (grow32(c, c->d_exts, c->exts_cap, std::max<uint32_t>(c->exts_cap, 1u << 17))) return PS4_ERR_CUDA;
+    if (grow32(c, c->d_sixes, c->sixes_cap, std::max<uint32_t>(c->sixes_cap, 1024))) return PS4_ERR_CUDA;
+    const int kernel = (int)c->cfg.kernel;
+    for (int attempt = 0; attempt < 16; attempt++) {
+        const unsigned TL = c->tile_log2;
+        tiles_total = 0;
+        for (uint32_t i = 0; i < n_items; i++) {
+            items[i].tile_base = tiles_total;
+            tiles_total += (items[i].hi - items[i].lo + (1ull << TL) - 1) >> TL;
+        }
+        if (tiles_total >= (1ull << 31))
+            return set_err(c, PS4_ERR_ARG, "range too large for one call (%llu tiles); split it",
+                           (unsigned long long)tiles_total);
+        const uint32_t quad_cap = quad_cap_for(TL);
+        int ctas_per_sm = c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1;
+        int grid = c->num_sms * ctas_per_sm;
+        if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
+        if (kernel == PS4_KERNEL_BATCHED) {
+            const size_t words = (size_t)grid * 6 * quad_cap;
+            uint64_t cap = c->scratch_words;
+            if (grow(c, c->d_scratch, cap, words)) return PS4_ERR_CUDA;
+            c->scratch_words = cap;
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_items, items.data(), n_items * sizeof(Item), cudaMemcpyHostToDevice,
+                                    c->stream));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long),
+                                    c->stream));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
+        SearchArgs a;
+        memset(&a, 0, sizeof a);
+        a.items = c->d_items; a.n_items = n_items; a.n_tiles = tiles_total; a.log2_tile = TL;
+        a.spfq = c->d_spfq; a.ndiv = c->d_ndiv; a.tab_n = c->tab_n;
+        a.counters = c->d_counters;
+        a.hits = c->d_hits; a.hits_cap = c->hits_cap;
+        a.exts = c->d_exts; a.exts_cap = c->exts_cap;
+        a.sixes = c->d_sixes; a.sixes_cap = c->sixes_cap;
+        a.quads = dump ? c->d_quads : nullptr; a.quads_cap = dump ? c->quads_cap : 0;
+        a.scratch = c->d_scratch; a.quad_cap = quad_cap;
+        a.status = c->d_status;
+        a.cap_reps = c->cfg.cap_reps; a.cap_divs = c->cfg.cap_divs; a.cap_ext = c->cfg.cap_ext;
+        a.flags = c->cfg.flags & (dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
+        if (tiles_total > 0) {
+            CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+            CUDA_TRY(c, (cudaError_t)launch_search(a, kernel, grid, c->stream));
+            CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+            c->last_launches++;
+        }
+        CUDA_TRY(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (tiles_total > 0) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            c->last_ms = ms;                     // the attempt whose results are kept
+        }
+        const Status &st = *c->h_status;
+        const unsigned code = (unsigned)(st.err & 0xFF);
+        const unsigned long long errS = st.err >> 8;
+        if (code == E_TILE || code == E_EXTLIST) {
+            if (c->tile_log2 > 12) { c->tile_log2--; continue; }
+            return set_err(c, PS4_ERR_CAP_REPS, "FATAL: tile capacity exceeded near S=%llu; this interval is NOT certified complete",
+                           errS);
+        }
+        if (code != 0) {
+            if (code == E_VERIFY)
+                return set_err(c, PS4_ERR_VERIFY, "BAD 4-set S=%llu [%lld,%lld,%lld,%lld]",
+                               st.verify_bad[0], (long long)st.verify_bad[1], (long long)st.verify_bad[2],
+                               (long long)st.verify_bad[3], (long long)st.verify_bad[4]);
+            return set_err(c, (int)code, "FATAL: %s; this interval is NOT certified complete", fatal_text(code));
+        }
+        bool regrow = false;
+        if (st.n_hits > c->hits_cap) { if (grow32(c, c->d_hits, c->hits_cap, (uint64_t)st.n_hits * 3 / 2 + 1024)) return PS4_ERR_CUDA; regrow = true; }
+        if (st.n_exts > c->exts_cap) { if (grow32(c, c->d_exts, c->exts_cap, (uint64_t)st.n_exts * 3 / 2 + 1024)) return PS4_ERR_CUDA; regrow = true; }
+        if (st.n_sixes > c->sixes_cap) { if (grow32(c, c->d_sixes, c->sixes_cap, (uint64_t)st.n_sixes * 3 / 2 + 64)) return PS4_ERR_CUDA; regrow = true; }
+        if (regrow) continue;
+        // results are complete on the device
+        if (res) {
+            res->n_quads = dump ? st.n_quads : 0;
+            if (dump && st.n_quads > res->quads_cap) {
+                res->n_hits = st.n_hits; res->n_exts = st.n_exts; res->n_sixes = st.n_sixes;
+                return set_err(c, PS4_ERR_OUTPUT_FULL, "dump4 buffer holds %llu 4-sets, %llu needed",
+                               (unsigned long long)res->quads_cap, st.n_quads);
+            }
+        }
+        // counters
+        std::vector<unsigned long long> k((size_t)n_items * K_SLOTS);
+        CUDA_TRY(c, cudaMemcpyAsync(k.data(), c->d_counters, k.size() * sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, c->stream));
+        std::vector<ps4_hit> hits(st.n_hits);
+        std::vector<ps4_ext> exts(st.n_exts);
+        std::vector<ps4_six> sixes(st.n_sixes);
+        if (st.n_hits) CUDA_TRY(c, cudaMemcpyAsync(hits.data(), c->d_hits, st.n_hits * sizeof(ps4_hit), cudaMemcpyDeviceToHost, c->stream));
+        if (st.n_exts) CUDA_TRY(c, cudaMemcpyAsync(exts.data(), c->d_exts, st.n_exts * sizeof(ps4_ext), cudaMemcpyDeviceToHost, c->stream));
+        if (st.n_sixes) CUDA_TRY(c, cudaMemcpyAsync(sixes.data(), c->d_sixes, st.n_sixes * sizeof(ps4_six), cudaMemcpyDeviceToHost, c->stream));
+        if (res && dump && st.n_quads)
+            CUDA_TRY(c, cudaMemcpyAsync(res->quads, c->d_quads, st.n_quads * sizeof(ps4_quad), cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        if (res) {
+            // deterministic order: item, S, then the reference's emission order (px, py, pz, class)
+            std::vector<uint32_t> perm(hits.size());
+            for (uint32_t i = 0; i < perm.size(); i++) perm[i] = i;
+            std::sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+                const ps4_hit &p = hits[x], &q = hits[y];
+                if (p.item != q.item) return p.item < q.item;
+                if (p.S != q.S) return p.S < q.S;
+                for (int i = 0; i < 4; i++)
+                    if (p.order[i] != q.order[i]) return p.order[i] < q.order[i];
+                return false;
+            });
+            res->n_hits = hits.size();
+            res->n_exts = exts.size();
+            res->n_sixes = sixes.size();
+            if (res->n_hits > res->hits_cap || res->n_exts > res->exts_cap || res->n_sixes > res->sixes_cap)
+                return set_err(c, PS4_ERR_OUTPUT_FULL, "result buffers too small: need hits=%llu exts=%llu sixes=%llu",
+                               (unsigned long long)res->n_hits, (unsigned long long)res->n_exts,
+                               (unsigned long long)res->n_sixes);
+            std::vector<uint32_t> newpos(hits.size());
+            uint32_t e = 0;
+            for (uint32_t i = 0; i < perm.size(); i++) {
+                ps4_hit h = hits[perm[i]];
+                newpos[perm[i]] = i;
+                for (uint32_t t = 0; t < h.n_ext; t++) res->exts[e + t] = exts[h.first_ext + t];
+                h.first_ext = e;
+                e += h.n_ext;
+                res->hits[i] = h;
+            }
+            std::vector<ps4_six> sx = sixes;
+            for (auto &s : sx) s.hit = newpos[s.hit];
+            std::sort(sx.begin(), sx.end(), [](const ps4_six &p, const ps4_six &q) {
+                if (p.hit != q.hit) return p.hit < q.hit;
+                if (p.t != q.t) return p.t < q.t;
+                return p.s < q.s;
+            });
+            for (size_t i = 0; i < sx.size(); i++) res->sixes[i] = sx[i];
+        }
+        if (stats)
+            for (uint32_t i = 0; i < n_items; i++) stats_add(&stats[i], &k[(size_t)i * K_SLOTS]);
+        return PS4_OK;
+    }
+    return set_err(c, PS4_ERR_CUDA, "search did not converge after repeated re-runs");
+}
+
+extern "C" int ps4_search_range(ps4_ctx *c, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res) {
+    if (!c) return PS4_ERR_ARG;
+    if (lo < 1) lo = 1;
+    if (hi < lo) hi = lo;
+    return run_items(c, &lo, &hi, 1, stats, res);
+}
+
+extern "C" int ps4_search_batch(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, ps4_stats *stats,
+                                ps4_results *res) {
+    if (!c || !lo || !hi || n_items == 0) return set_err(c, PS4_ERR_ARG, "ps4_search_batch: empty batch");
+    return run_items(c, lo, hi, n_items, stats, res);
+}

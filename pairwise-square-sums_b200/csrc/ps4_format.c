@@ -1,0 +1,119 @@
+/*
+ * ps4_format.c -- result-line text of the C-ABI, byte-identical to the reference's
+ * output (exhaustive/s4.c:24-27): "M:" lines (s4.c:250-253), "5:" / 6-set / drill lines
+ * through format_set (s4.c:214-220), "4:" dump lines (s4.c:239).
+ *
+ * Pure formatting: every number and every verify flag comes from the device records.
+ */
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/ps4.h"
+
+typedef unsigned __int128 u128;
+
+typedef struct { char *p; size_t cap, len; int bad; } sbuf;
+
+static void put(sbuf *b, const char *s, size_t n) {
+    if (b->bad || b->len + n + 1 > b->cap) { b->bad = 1; return; }
+    memcpy(b->p + b->len, s, n);
+    b->len += n;
+    b->p[b->len] = 0;
+}
+static void puts_(sbuf *b, const char *s) { put(b, s, strlen(s)); }
+
+static void put_u128(sbuf *b, u128 v) {
+    char tmp[48];
+    int i = 0;
+    if (v == 0) { put(b, "0", 1); return; }
+    while (v) { tmp[i++] = (char)('0' + (int)(v % 10)); v /= 10; }
+    char out[48];
+    for (int j = 0; j < i; j++) out[j] = tmp[i - 1 - j];
+    put(b, out, (size_t)i);
+}
+static void put_u64(sbuf *b, unsigned long long v) { put_u128(b, (u128)v); }
+
+static u128 ext_value(const ps4_ext *e) { return ((u128)e->hi << 64) | e->lo; }
+
+/* "tag [x sorted descending] S=...<verify note>\n" */
+static void put_set(sbuf *b, const char *tag, u128 *x, int n, uint64_t S, int verified) {
+    for (int i = 0; i < n; i++)
+        for (int j = i + 1; j < n; j++)
+            if (x[j] > x[i]) { u128 t = x[i]; x[i] = x[j]; x[j] = t; }
+    puts_(b, tag);
+    puts_(b, " [");
+    for (int i = 0; i < n; i++) {
+        put_u128(b, x[i]);
+        if (i < n - 1) put(b, ",", 1);
+    }
+    puts_(b, "] S=");
+    put_u64(b, S);
+    if (!verified) puts_(b, "  *** VERIFY FAILED ***");
+    put(b, "\n", 1);
+}
+
+static long done(sbuf *b) { return b->bad ? -1 : (long)b->len; }
+
+long ps4_format_hit(const ps4_hit *h, const ps4_ext *exts, char *buf, size_t cap) {
+    sbuf b = {buf, cap, 0, cap == 0};
+    if (cap) buf[0] = 0;
+    const ps4_ext *e = exts + h->first_ext;
+    if (h->n_ext >= 2) {
+        puts_(&b, "M: [");
+        for (int i = 0; i < 4; i++) { put_u64(&b, h->v[i]); if (i < 3) put(&b, ",", 1); }
+        puts_(&b, "] ext=[");
+        for (uint32_t t = 0; t < h->n_ext; t++) {
+            put_u128(&b, ext_value(&e[t]));
+            if (t + 1 < h->n_ext) put(&b, ",", 1);
+        }
+        puts_(&b, "] S=");
+        put_u64(&b, h->S);
+        put(&b, "\n", 1);
+    }
+    for (uint32_t t = 0; t < h->n_ext; t++) {
+        if (!(e[t].flags & PS4_EXT_FIVE)) continue;
+        u128 x[5] = {h->v[0], h->v[1], h->v[2], h->v[3], ext_value(&e[t])};
+        put_set(&b, "5:", x, 5, h->S, (e[t].flags & PS4_EXT_FIVE_OK) != 0);
+    }
+    return done(&b);
+}
+
+long ps4_format_six(const ps4_hit *h, const ps4_ext *exts, const ps4_six *s, char *buf, size_t cap) {
+    sbuf b = {buf, cap, 0, cap == 0};
+    if (cap) buf[0] = 0;
+    const ps4_ext *e = exts + h->first_ext;
+    u128 x[6] = {h->v[0], h->v[1], h->v[2], h->v[3], ext_value(&e[s->t]), ext_value(&e[s->s])};
+    put_set(&b, "!!!!!!!! FOUND 6-SET:", x, 6, h->S, (s->flags & 1) != 0);
+    return done(&b);
+}
+
+long ps4_format_drill(const ps4_hit *h, const ps4_ext *exts, char *buf, size_t cap) {
+    sbuf b = {buf, cap, 0, cap == 0};
+    if (cap) buf[0] = 0;
+    if (h->n_ext < 2) return 0;
+    const ps4_ext *e = exts + h->first_ext;
+    u128 x[6] = {h->v[0], h->v[1], h->v[2], h->v[3], ext_value(&e[0]), ext_value(&e[1])};
+    put_set(&b, "TEST-6SET (NOT A SOLUTION, --test-sixset drill):", x, 6, h->S, (h->flags & PS4_HIT_DRILL_OK) != 0);
+    return done(&b);
+}
+
+void ps4_quad_values(const ps4_quad *q, uint64_t *S, uint64_t v[4], uint32_t order[4]) {
+    uint64_t ab = (uint64_t)q->r_ab * q->r_ab, ac = (uint64_t)q->r_ac * q->r_ac, ad = (uint64_t)q->r_ad * q->r_ad;
+    uint64_t bc = (uint64_t)q->r_bc * q->r_bc, cd = (uint64_t)q->r_cd * q->r_cd;
+    uint64_t a = (ab + ac - bc) >> 1;
+    v[0] = a; v[1] = ab - a; v[2] = ac - a; v[3] = ad - a;
+    *S = ab + cd;
+    order[0] = q->r_cd;                                   /* p of representation x */
+    order[1] = q->r_bd;                                   /* p of representation y */
+    order[2] = q->r_ad < q->r_bc ? q->r_ad : q->r_bc;      /* p of representation z */
+    order[3] = q->r_ad < q->r_bc ? 1u : 0u;                /* class */
+}
+
+long ps4_format_quad(const ps4_quad *q, char *buf, size_t cap) {
+    uint64_t S, v[4];
+    uint32_t order[4];
+    ps4_quad_values(q, &S, v, order);
+    int n = snprintf(buf, cap, "4: [%lld,%lld,%lld,%lld] S=%llu\n", (long long)v[0], (long long)v[1], (long long)v[2],
+                     (long long)v[3], (unsigned long long)S);
+    return (n < 0 || (size_t)n >= cap) ? -1 : n;
+}

@@ -1,0 +1,75 @@
+// ps4_internal.h -- layouts shared by the device kernels (ps4_kernels.cu) and the host
+// orchestration behind the C-ABI (ps4_api.cu).  Not part of the public interface.
+#pragma once
+#include <stdint.h>
+
+#include "../../include/ps4.h"
+
+namespace ps4 {
+
+// ---- per-item counter block (u64 slots), one block per query item -------------------
+// Slots 0..9 are the reference's additive counters in stats_t order (s4.c:81), 10..12
+// the capacity high-water marks (s4.c:90), 16..115 the 5-set log2 histogram (s4.c:82).
+enum {
+    K_S_DONE = 0, K_PAIRS, K_S_GE3, K_TRIPLES, K_SETS4, K_SETS5, K_SETS6, K_MULTI, K_EXT_CAND, K_EXT_SQRT,
+    K_MAX_REPS = 10, K_MAX_DIVS = 11, K_MAX_EXT = 12,
+    K_HIST5 = 16,
+    K_SLOTS = 128
+};
+
+// ---- device error word: code in bits 0..7, the S where it happened in bits 8..63 -----
+enum {
+    E_NONE = 0,
+    E_CAP_REPS = PS4_ERR_CAP_REPS,
+    E_CAP_DIVS = PS4_ERR_CAP_DIVS,
+    E_CAP_EXT = PS4_ERR_CAP_EXT,
+    E_VERIFY = PS4_ERR_VERIFY,
+    E_TILE = 100,      // a tile outgrew its shared-memory lists: re-run with smaller tiles
+    E_EXTLIST = 101    // more extensions in one tile than the per-tile list holds: re-run smaller
+};
+
+// One query item: every S in [lo, hi).  Tiles of the item are numbered from tile_base.
+struct Item {
+    uint64_t lo, hi;
+    uint64_t tile_base;   // prefix sum of tile counts over the items before this one
+};
+
+// Status block copied back after every launch.
+struct Status {
+    unsigned long long err;        // first error (code | S << 8)
+    unsigned long long verify_bad[5];  // --verify failure: S, a, b, c, d
+    unsigned int n_hits, n_exts, n_sixes, pad0;
+    unsigned long long n_quads;
+    unsigned int tile_next;        // persistent-kernel work counter
+    unsigned int pad1;
+};
+
+// Arguments of one search launch (passed by value).
+struct SearchArgs {
+    const Item *items;
+    uint32_t n_items;
+    uint64_t n_tiles;
+    unsigned log2_tile;
+    const uint64_t *spfq;      // spf | quot << 32, m < tab_n
+    const uint16_t *ndiv;      // divisor counts, m < tab_n
+    uint64_t tab_n;
+    unsigned long long *counters;   // [n_items][K_SLOTS]
+    ps4_hit *hits;   uint32_t hits_cap;
+    ps4_ext *exts;   uint32_t exts_cap;
+    ps4_six *sixes;  uint32_t sixes_cap;
+    ps4_quad *quads; unsigned long long quads_cap;
+    uint32_t *scratch;         // per-CTA 4-set staging (batched kernel): 6 * quad_cap u32 per CTA
+    uint32_t quad_cap;         // 4-sets per tile the staging holds
+    Status *status;
+    uint32_t cap_reps, cap_divs, cap_ext;
+    uint32_t flags;            // PS4_F_*
+};
+
+// Launchers (ps4_kernels.cu).  Return a cudaError_t value.
+int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream);
+int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);
+size_t search_smem_bytes(int kernel, unsigned log2_tile);
+int search_block_threads();
+uint32_t quad_cap_for(unsigned log2_tile);
+
+}  // namespace ps4

@@ -1,0 +1,168 @@
+"""Python face of the search: one object per device context, mirroring the reference's
+process interface (exhaustive/s4.c) as calls.
+
+``Search(s_hi_max).range(lo, hi)`` returns what one ``s4 lo hi`` invocation reports: the
+counters of its TOTAL / CAPACITY lines (s4.c:498-506) and its result lines (s4.c:24-27),
+byte-identical in text.  Every call goes through the C-ABI of lib/libps4.so; the numbers
+are computed on the GPU only.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+from . import _abi
+
+_LINE_CAP = 1 << 16
+
+
+class Ps4Error(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+        self.message = message
+
+
+@dataclass
+class RangeResult:
+    stats: dict
+    lines: list = field(default_factory=list)      # "M:" and "5:" lines, reference order
+    six_lines: list = field(default_factory=list)  # "!!!!!!!! FOUND 6-SET:" alert lines
+    quads: list = field(default_factory=list)      # "4:" lines (dump4 mode)
+    items: list = field(default_factory=list)      # item index of each entry of `lines`
+    kernel_ms: float = 0.0
+
+
+def _alloc(kind, n):
+    n = max(int(n), 1)
+    return (kind * n)(), n
+
+
+class Search:
+    """A device context (tables for S < s_hi_max) and its search calls."""
+
+    def __init__(self, s_hi_max: int, device: int = 0, *, noext: bool = False, verify: bool = False,
+                 dump4: bool = False, kernel: str = "batched", cap_reps: int = 0, cap_divs: int = 0,
+                 cap_ext: int = 0, log2_tile: int = 0, ctas_per_sm: int = 0, stream: int | None = None):
+        self.lib = _abi.load()
+        cfg = _abi.Config()
+        cfg.device = device
+        cfg.s_hi_max = int(s_hi_max)
+        cfg.cap_reps, cfg.cap_divs, cfg.cap_ext = cap_reps, cap_divs, cap_ext
+        cfg.flags = ((_abi.PS4_F_NOEXT if noext else 0) | (_abi.PS4_F_VERIFY if verify else 0)
+                     | (_abi.PS4_F_DUMP4 if dump4 else 0))
+        cfg.kernel = {"batched": _abi.PS4_KERNEL_BATCHED, "plain": _abi.PS4_KERNEL_PLAIN}[kernel]
+        cfg.log2_tile = log2_tile
+        cfg.ctas_per_sm = ctas_per_sm
+        cfg.stream = stream
+        self.dump4 = dump4
+        self.ctx = C.c_void_p()
+        rc = self.lib.ps4_create(C.byref(cfg), C.byref(self.ctx))
+        if rc != _abi.PS4_OK:
+            msg = self.lib.ps4_last_error(self.ctx).decode() if self.ctx else "ps4_create failed"
+            self.close()
+            raise Ps4Error(rc, msg)
+        self._res = _abi.Results()
+        self._hits, self._res.hits_cap = _alloc(_abi.Hit, 1 << 12)
+        self._exts, self._res.exts_cap = _alloc(_abi.Ext, 1 << 13)
+        self._sixes, self._res.sixes_cap = _alloc(_abi.Six, 64)
+        self._quads, self._res.quads_cap = _alloc(_abi.Quad, (1 << 16) if dump4 else 1)
+        self._bind()
+
+    def _bind(self):
+        r = self._res
+        r.hits = C.cast(self._hits, C.POINTER(_abi.Hit))
+        r.exts = C.cast(self._exts, C.POINTER(_abi.Ext))
+        r.sixes = C.cast(self._sixes, C.POINTER(_abi.Six))
+        r.quads = C.cast(self._quads, C.POINTER(_abi.Quad))
+        if not self.dump4:
+            r.quads_cap = 0
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.lib.ps4_destroy(self.ctx)
+            self.ctx = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def last_kernel_ms(self) -> float:
+        return float(self.lib.ps4_last_kernel_ms(self.ctx))
+
+    @property
+    def last_launches(self) -> int:
+        return int(self.lib.ps4_last_launches(self.ctx))
+
+    def _grow(self):
+        r = self._res
+        if r.n_hits > r.hits_cap:
+            self._hits, r.hits_cap = _alloc(_abi.Hit, r.n_hits * 3 // 2)
+        if r.n_exts > r.exts_cap:
+            self._exts, r.exts_cap = _alloc(_abi.Ext, r.n_exts * 3 // 2)
+        if r.n_sixes > r.sixes_cap:
+            self._sixes, r.sixes_cap = _alloc(_abi.Six, r.n_sixes * 3 // 2)
+        if self.dump4 and r.n_quads > r.quads_cap:
+            self._quads, r.quads_cap = _alloc(_abi.Quad, r.n_quads * 3 // 2)
+        self._bind()
+
+    def _call(self, fn):
+        while True:
+            rc = fn()
+            if rc == _abi.PS4_ERR_OUTPUT_FULL:
+                self._grow()
+                continue
+            if rc != _abi.PS4_OK:
+                raise Ps4Error(rc, self.lib.ps4_last_error(self.ctx).decode())
+            return
+
+    def range(self, lo: int, hi: int, *, want_lines: bool = True) -> RangeResult:
+        """Every S in [lo, hi): counters and result lines (one reference invocation)."""
+        st = _abi.Stats()
+        self._call(lambda: self.lib.ps4_search_range(self.ctx, lo, hi, C.byref(st), C.byref(self._res)))
+        out = RangeResult(stats=st.as_dict(), kernel_ms=self.last_kernel_ms)
+        if want_lines:
+            self._collect(out)
+        return out
+
+    def batch(self, los, his, *, want_lines: bool = True):
+        """Many subranges in one launch: (per-item stats list, RangeResult with item tags)."""
+        n = len(los)
+        lo_arr = (C.c_uint64 * n)(*los)
+        hi_arr = (C.c_uint64 * n)(*his)
+        st = (_abi.Stats * n)()
+        self._call(lambda: self.lib.ps4_search_batch(self.ctx, lo_arr, hi_arr, n, st, C.byref(self._res)))
+        out = RangeResult(stats={}, kernel_ms=self.last_kernel_ms)
+        if want_lines:
+            self._collect(out)
+        return [s.as_dict() for s in st], out
+
+    def _collect(self, out: RangeResult):
+        r = self._res
+        buf = C.create_string_buffer(_LINE_CAP)
+        for i in range(r.n_hits):
+            h = C.byref(self._hits[i])
+            n = self.lib.ps4_format_hit(h, self._exts, buf, _LINE_CAP)
+            if n > 0:
+                for line in buf.value.decode().splitlines(keepends=True):
+                    out.lines.append(line)
+                    out.items.append(self._hits[i].item)
+        for s in range(r.n_sixes):
+            six = self._sixes[s]
+            n = self.lib.ps4_format_six(C.byref(self._hits[six.hit]), self._exts, C.byref(six), buf, _LINE_CAP)
+            if n > 0:
+                out.six_lines.append(buf.value.decode())
+        if self.dump4:
+            for q in range(r.n_quads):
+                n = self.lib.ps4_format_quad(C.byref(self._quads[q]), buf, _LINE_CAP)
+                if n > 0:
+                    out.quads.append(buf.value.decode())
