@@ -1,0 +1,331 @@
+#!/usr/bin/env python3
+"""Benchmark: the exhaustive square-sum search over S in [1, 1e10) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--kernel batched|plain]
+
+One step = one complete search of the rank's S range (the reference's `s4 1 10000000000`):
+every 4-set with S below the bound, every extension, every counter.  N > 1 runs under
+torchrun, one process per GPU; each rank searches its own 1e10-wide shard
+[r*1e10, (r+1)*1e10) (weak scaling, no data-path collective; the time is the max over
+ranks).  Rank 0 prints one JSON line.
+
+value      S covered per second with the work enqueued on the device (CUDA events on the
+           launch stream around each step; a 256 MiB write flushes L2 between steps,
+           outside the events)
+e2e        the same through the public C-ABI call with host result buffers
+           (ps4_search_range: input copy, search, result copies, host collection)
+roofline   integer-issue roofline: algorithmic int32 lane-ops per launch (ps4b200/opmodel.py,
+           frozen) / kernel time, against 4 warp-instructions x 32 lanes per SM per clock
+cpu_baseline  the reference's own s4 (oracle/_ref/s4, all host threads) on a stratified
+           sample of the same range, timed on this host
+--impl reference  that CPU reference alone, as the reference arm
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "pairwise-square-sums_b200"))
+
+BOUND = 10 ** 10
+METRIC = "range_per_s"
+UNIT = "S/s"
+
+
+def shard(rank: int) -> tuple[int, int]:
+    """Rank r searches S in [max(1, r*B), (r+1)*B): rank 0 is the s4 bound-1e10 workload."""
+    return max(1, rank * BOUND), (rank + 1) * BOUND
+
+
+# ------------------------------------------------------------------ CPU reference (s4)
+
+def _s4_binary():
+    ref = REPO / "oracle" / "_ref" / "s4"
+    if ref.exists():
+        return ref, "reference"
+    port = REPO / "oracle" / "ps4_oracle"
+    return port, "port"
+
+
+def _run_s4(binary: Path, kind: str, lo: int, hi: int, threads: int) -> float:
+    """Seconds of search work for one s4 run: the slowest region thread's own timer (the
+    process wall time adds s4's 1 s polling granularity, s4.c:470-474)."""
+    if kind == "reference":
+        t0 = time.perf_counter()
+        p = subprocess.run([str(binary), str(lo), str(hi), str(threads), "20"], capture_output=True, text=True,
+                           check=True)
+        wall = time.perf_counter() - t0
+        secs = [float(x) for x in re.findall(r"^\s+thread\s+\d+: .*?\s([\d.]+)s$", p.stderr, re.M)]
+        return max(secs) if secs and max(secs) > 0 else wall
+    t0 = time.perf_counter()
+    subprocess.run([str(binary), str(lo), str(hi)], capture_output=True, text=True, check=True)
+    return time.perf_counter() - t0
+
+
+def _strata(width: int, lo: int, hi: int, k: int = 4):
+    """k slices of `width` centred at the midpoints of k equal parts of [lo, hi)."""
+    span = hi - lo
+    return [(lo + span * (2 * j + 1) // (2 * k) - width // 2, lo + span * (2 * j + 1) // (2 * k) - width // 2 + width)
+            for j in range(k)]
+
+
+def cpu_sample_plan(lo: int, hi: int, budget_s: float):
+    binary, kind = _s4_binary()
+    threads = (os.cpu_count() or 1) if kind == "reference" else 1
+    w0 = 2 * 10 ** 7
+    mid = (lo + hi) // 2
+    t = _run_s4(binary, kind, mid, mid + w0, threads)
+    rate = w0 / max(t, 1e-3)
+    width = int(max(10 ** 6, min((hi - lo) // 8, rate * budget_s / 4)))
+    return binary, kind, threads, _strata(width, lo, hi)
+
+
+def cpu_sample_run(binary, kind, threads, slices) -> tuple[float, int]:
+    secs = sum(_run_s4(binary, kind, a, b, threads) for a, b in slices)
+    return secs, sum(b - a for a, b in slices)
+
+
+def run_reference(args, rank: int):
+    """The reference arm: s4 itself on this host's cores, on a bounded sample of the workload."""
+    if rank != 0:
+        return
+    lo, hi = shard(0)
+    binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=args.ref_budget)
+    for _ in range(args.warmup):
+        cpu_sample_run(binary, kind, threads, slices)
+    total_s, total_S = 0.0, 0
+    for _ in range(args.steps):
+        s, n = cpu_sample_run(binary, kind, threads, slices)
+        total_s += s
+        total_S += n
+    value = total_S / total_s
+    sample = f"{len(slices)} slices of {slices[0][1] - slices[0][0]} S at the midpoints of 4 equal parts of [1,1e10)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "exhaustive",
+            "config": {"workload": "exhaustive square-sum search, S in [1,1e10) (s4 bound 1e10), sampled",
+                       "bound": BOUND, "sample": sample},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    Q = ("uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and (not self.uuid or self.uuid in f[0]):
+                self.rows.append(f)
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(self.rows[0][2]) if self.rows[0][2].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ our arm
+
+def read_traffic_per_S():
+    p = REPO / "profiles" / "ncu_search_batched.txt"
+    if not p.exists():
+        return None
+    m = re.search(r"^dram_bytes_per_S:\s*([\d.eE+-]+)", p.read_text(), re.M)
+    return float(m.group(1)) if m else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--kernel", choices=["batched", "plain"], default="batched")
+    ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of s4 work per reference step")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--range", type=int, nargs=2, default=None, metavar=("LO", "HI"),
+                    help="search [LO, HI) instead of the rank's shard (a smaller case for ncu captures)")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank)
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    from ps4b200 import Search, opmodel
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    lo, hi = shard(rank) if args.range is None else tuple(args.range)
+    # one dedicated stream carries the library's launches, the L2 flush and the timing events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    s = Search(hi, device=local, kernel=args.kernel, stream=stream.cuda_stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    props = torch.cuda.get_device_properties(local)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        s.enqueue(lo, hi)
+        s.finish(want_lines=False)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(str(getattr(props, "uuid", "")))
+    clocks.start()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    kernel_ms, stats, launches = [], None, 0
+    for i in range(args.steps):
+        flush.zero_()                                  # L2 flush, outside the timed events
+        ev[i][0].record(stream)
+        s.enqueue(lo, hi)
+        ev[i][1].record(stream)
+        r = s.finish(want_lines=False)
+        kernel_ms.append(r.kernel_ms)
+        launches += s.last_launches
+        stats = r.stats
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    dev_s = sum(a.elapsed_time(b) for a, b in ev) / 1000.0
+    kern_s = sum(kernel_ms) / 1000.0
+    S_rank = (hi - lo) * args.steps
+    cand_rank = stats["ext_cand"] * args.steps
+    ops_launch = opmodel.ops(stats)
+
+    # e2e: the public C-ABI call with host buffers, input copy + result copies inside
+    torch.cuda.synchronize()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    h2d = d2h = 0
+    e2e_lines = 0
+    for _ in range(args.steps):
+        rr = s.range(lo, hi)
+        a_, b_ = s.transfer_bytes()
+        h2d += a_
+        d2h += b_
+        e2e_lines = len(rr.lines)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    e2e_s = e0.elapsed_time(e1) / 1000.0
+
+    vals = torch.tensor([dev_s, e2e_s, kern_s], dtype=torch.float64, device="cuda")
+    tot = torch.tensor([S_rank, cand_rank], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    dev_s, e2e_s, kern_s = vals.tolist()
+    S_all, cand_all = tot.tolist()
+
+    plain = None
+    if world == 1 and args.kernel == "batched" and not args.no_plain:
+        with Search(hi, device=local, kernel="plain", stream=stream.cuda_stream) as sp:
+            sp.enqueue(lo, hi)
+            sp.finish(want_lines=False)
+            flush.zero_()
+            pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            pe0.record(stream)
+            sp.enqueue(lo, hi)
+            pe1.record(stream)
+            pr = sp.finish(want_lines=False)
+            torch.cuda.synchronize()
+            assert pr.stats == stats, "plain and batched kernels disagree"
+            pt = pe0.elapsed_time(pe1) / 1000.0
+            plain = {"value": (hi - lo) / pt, "unit": UNIT, "ms_per_step": 1000 * pt,
+                     "batched_over_plain": ((hi - lo) / (dev_s / args.steps)) / ((hi - lo) / pt)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=4.0)
+        secs, n = cpu_sample_run(binary, kind, threads, slices)
+        cpu = {"value": n / secs, "unit": UNIT, "cores": threads, "kind": kind,
+               "sample": f"{len(slices)} slices of {slices[0][1] - slices[0][0]} S at the midpoints of 4 equal "
+                         f"parts of [1,1e10), slowest region thread's own timer"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    sm_hz = (clk["sm_mhz"] or 1965.0) * 1e6
+    peak = opmodel.issue_peak_lane_ops(props.multi_processor_count, sm_hz)
+    achieved = ops_launch / (kern_s / args.steps)
+    traffic_per_S = read_traffic_per_S()
+    line = {
+        "metric": METRIC, "value": S_all / dev_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "exhaustive",
+        "config": {"workload": "exhaustive square-sum 4-set search + extension, S in [r*1e10, (r+1)*1e10) "
+                               "per rank (s4 bound 1e10 on rank 0)",
+                   "bound_per_rank": BOUND, "kernel": args.kernel, "l2": "256 MiB write between timed steps",
+                   "parallelism": f"S shards x{world}"},
+        "candidates_per_s": cand_all / dev_s,
+        "sets4_per_s": stats["sets4"] * world * args.steps / dev_s,
+        "kernel_ms_per_step": 1000 * kern_s / args.steps,
+        "roofline": {"bound": "int_issue", "achieved": achieved, "peak": peak, "unit": "lane-op/s",
+                     "frac": achieved / peak,
+                     "peak_source": f"{props.multi_processor_count} SMs x 128 lanes x median SM clock under load "
+                                    f"({sm_hz / 1e6:.0f} MHz sampled); MEASURED_PEAKS.json has no integer peak",
+                     "ops_per_launch": ops_launch,
+                     "traffic": traffic_per_S * (hi - lo) if traffic_per_S else None},
+        "e2e": {"value": S_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": d2h // args.steps, "result_lines": e2e_lines},
+        "gpu_launches": launches,
+        "clocks": clk,
+        "plain_gpu": plain,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -136,6 +136,16 @@ int ps4_search_range(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, p
 int ps4_search_batch(ps4_ctx *ctx, const uint64_t *lo, const uint64_t *hi, uint32_t n_items,
                      ps4_stats *stats, ps4_results *res);
 
+/* The same search split in two: enqueue on the context's stream and return at once (no
+ * result copies), then wait, check and collect.  Lets a caller overlap host work with the
+ * device search, or time the device work alone with events on the stream.  At most one
+ * search may be enqueued per context.  (Same reference code as ps4_search_range.) */
+int ps4_search_enqueue(ps4_ctx *ctx, uint64_t lo, uint64_t hi);
+int ps4_search_finish(ps4_ctx *ctx, ps4_stats *stats, ps4_results *res);
+
+/* Bytes copied host->device and device->host by the last search call (inputs and results). */
+void ps4_last_transfer_bytes(const ps4_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
+
 /* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
 double ps4_last_kernel_ms(const ps4_ctx *ctx);
 /* Number of kernel launches made by the last search call. */

@@ -19,6 +19,13 @@
 
 using namespace ps4;
 
+struct PendingSearch {
+    std::vector<Item> items;
+    bool dump = false;
+    bool active = false;
+    uint64_t tiles = 0;
+};
+
 struct ps4_ctx {
     ps4_config cfg;
     cudaStream_t stream = nullptr;
@@ -41,6 +48,8 @@ struct ps4_ctx {
     double last_ms = 0.0;
     uint64_t last_launches = 0;
     unsigned tile_log2 = 14;             // current tile size (may shrink on E_TILE)
+    PendingSearch pend;
+    uint64_t h2d_bytes = 0, d2h_bytes = 0;
     std::string err;
 };
 
@@ -173,78 +182,104 @@ static const char *fatal_text(unsigned code) {
     }
 }
 
-// Run the search over n items (each [lo,hi)) in one launch, re-running on internal
-// capacity limits; results land in the device buffers.  stats: one per item (+=).
-static int run_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, ps4_stats *stats,
-                     ps4_results *res) {
-    std::vector<Item> items(n_items);
+// ---- one search = enqueue (host prep + launch, no wait) + finish (wait, check, collect) ----
+
+static int enqueue_items(ps4_ctx *c) {
+    PendingSearch &p = c->pend;
+    const uint32_t n_items = (uint32_t)p.items.size();
+    const unsigned TL = c->tile_log2;
     uint64_t tiles_total = 0;
+    for (uint32_t i = 0; i < n_items; i++) {
+        p.items[i].tile_base = tiles_total;
+        tiles_total += (p.items[i].hi - p.items[i].lo + (1ull << TL) - 1) >> TL;
+    }
+    if (tiles_total >= (1ull << 31))
+        return set_err(c, PS4_ERR_ARG, "range too large for one call (%llu tiles); split it",
+                       (unsigned long long)tiles_total);
+    p.tiles = tiles_total;
+    const int kernel = (int)c->cfg.kernel;
+    const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
+    int ctas_per_sm = c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1;
+    int grid = c->num_sms * ctas_per_sm;
+    if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
+    if (kernel == PS4_KERNEL_BATCHED) {
+        uint64_t cap = c->scratch_words;
+        if (grow(c, c->d_scratch, cap, (uint64_t)grid * 6 * stage_cap)) return PS4_ERR_CUDA;
+        c->scratch_words = cap;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_items, p.items.data(), n_items * sizeof(Item), cudaMemcpyHostToDevice,
+                                c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long),
+                                c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
+    c->h2d_bytes += n_items * sizeof(Item);
+    SearchArgs a;
+    memset(&a, 0, sizeof a);
+    a.items = c->d_items; a.n_items = n_items; a.n_tiles = tiles_total; a.log2_tile = TL;
+    a.spfq = c->d_spfq; a.ndiv = c->d_ndiv; a.tab_n = c->tab_n;
+    a.counters = c->d_counters;
+    a.hits = c->d_hits; a.hits_cap = c->hits_cap;
+    a.exts = c->d_exts; a.exts_cap = c->exts_cap;
+    a.sixes = c->d_sixes; a.sixes_cap = c->sixes_cap;
+    a.quads = p.dump ? c->d_quads : nullptr; a.quads_cap = p.dump ? c->quads_cap : 0;
+    a.scratch = c->d_scratch; a.stage_cap = stage_cap;
+    a.status = c->d_status;
+    a.cap_reps = c->cfg.cap_reps; a.cap_divs = c->cfg.cap_divs; a.cap_ext = c->cfg.cap_ext;
+    a.flags = c->cfg.flags & (p.dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
+    if (tiles_total > 0) {
+        CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+        CUDA_TRY(c, (cudaError_t)launch_search(a, kernel, grid, c->stream));
+        CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+        c->last_launches++;
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
+    return PS4_OK;
+}
+
+static int begin_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, bool want_dump,
+                       uint64_t dump_cap) {
+    if (c->pend.active) return set_err(c, PS4_ERR_ARG, "a search is already enqueued on this context");
+    PendingSearch &p = c->pend;
+    p.items.assign(n_items, Item{});
     c->last_launches = 0;
     c->last_ms = 0.0;
+    c->h2d_bytes = c->d2h_bytes = 0;
     for (uint32_t i = 0; i < n_items; i++) {
         uint64_t a = std::max<uint64_t>(lo[i], 1), b = hi[i];
         if (b > c->cfg.s_hi_max)
             return set_err(c, PS4_ERR_ARG, "S_hi %llu exceeds the context's s_hi_max %llu", (unsigned long long)b,
                            (unsigned long long)c->cfg.s_hi_max);
         if (b < a) b = a;
-        items[i].lo = a;
-        items[i].hi = b;
+        p.items[i].lo = a;
+        p.items[i].hi = b;
     }
     if (grow32(c, c->d_items, c->items_cap, n_items)) return PS4_ERR_CUDA;
     if (grow32(c, c->d_counters, c->counters_items, (uint64_t)n_items * K_SLOTS)) return PS4_ERR_CUDA;
-    const bool dump = (c->cfg.flags & PS4_F_DUMP4) && res && res->quads_cap > 0;
-    if (dump && grow(c, c->d_quads, c->quads_cap, res->quads_cap)) return PS4_ERR_CUDA;
+    p.dump = (c->cfg.flags & PS4_F_DUMP4) && want_dump && dump_cap > 0;
+    if (p.dump && grow(c, c->d_quads, c->quads_cap, dump_cap)) return PS4_ERR_CUDA;
     if (grow32(c, c->d_hits, c->hits_cap, std::max<uint32_t>(c->hits_cap, 1u << 16))) return PS4_ERR_CUDA;
     if (grow32(c, c->d_exts, c->exts_cap, std::max<uint32_t>(c->exts_cap, 1u << 17))) return PS4_ERR_CUDA;
     if (grow32(c, c->d_sixes, c->sixes_cap, std::max<uint32_t>(c->sixes_cap, 1024))) return PS4_ERR_CUDA;
-    const int kernel = (int)c->cfg.kernel;
+    int rc = enqueue_items(c);
+    if (rc == PS4_OK) p.active = true;
+    return rc;
+}
+
+// Wait for the enqueued search, re-run it on internal capacity limits, then copy the results
+// into the caller's buffers and add the counters (stats: one per item, +=).
+static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
+    PendingSearch &p = c->pend;
+    if (!p.active) return set_err(c, PS4_ERR_ARG, "no search enqueued on this context");
+    p.active = false;
+    const uint32_t n_items = (uint32_t)p.items.size();
     for (int attempt = 0; attempt < 16; attempt++) {
-        const unsigned TL = c->tile_log2;
-        tiles_total = 0;
-        for (uint32_t i = 0; i < n_items; i++) {
-            items[i].tile_base = tiles_total;
-            tiles_total += (items[i].hi - items[i].lo + (1ull << TL) - 1) >> TL;
+        if (attempt > 0) {
+            int rc = enqueue_items(c);
+            if (rc) return rc;
         }
-        if (tiles_total >= (1ull << 31))
-            return set_err(c, PS4_ERR_ARG, "range too large for one call (%llu tiles); split it",
-                           (unsigned long long)tiles_total);
-        const uint32_t quad_cap = quad_cap_for(TL);
-        int ctas_per_sm = c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1;
-        int grid = c->num_sms * ctas_per_sm;
-        if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
-        if (kernel == PS4_KERNEL_BATCHED) {
-            const size_t words = (size_t)grid * 6 * quad_cap;
-            uint64_t cap = c->scratch_words;
-            if (grow(c, c->d_scratch, cap, words)) return PS4_ERR_CUDA;
-            c->scratch_words = cap;
-        }
-        CUDA_TRY(c, cudaMemcpyAsync(c->d_items, items.data(), n_items * sizeof(Item), cudaMemcpyHostToDevice,
-                                    c->stream));
-        CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long),
-                                    c->stream));
-        CUDA_TRY(c, cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
-        SearchArgs a;
-        memset(&a, 0, sizeof a);
-        a.items = c->d_items; a.n_items = n_items; a.n_tiles = tiles_total; a.log2_tile = TL;
-        a.spfq = c->d_spfq; a.ndiv = c->d_ndiv; a.tab_n = c->tab_n;
-        a.counters = c->d_counters;
-        a.hits = c->d_hits; a.hits_cap = c->hits_cap;
-        a.exts = c->d_exts; a.exts_cap = c->exts_cap;
-        a.sixes = c->d_sixes; a.sixes_cap = c->sixes_cap;
-        a.quads = dump ? c->d_quads : nullptr; a.quads_cap = dump ? c->quads_cap : 0;
-        a.scratch = c->d_scratch; a.quad_cap = quad_cap;
-        a.status = c->d_status;
-        a.cap_reps = c->cfg.cap_reps; a.cap_divs = c->cfg.cap_divs; a.cap_ext = c->cfg.cap_ext;
-        a.flags = c->cfg.flags & (dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
-        if (tiles_total > 0) {
-            CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-            CUDA_TRY(c, (cudaError_t)launch_search(a, kernel, grid, c->stream));
-            CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
-            c->last_launches++;
-        }
-        CUDA_TRY(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-        if (tiles_total > 0) {
+        c->d2h_bytes += sizeof(Status);
+        if (p.tiles > 0) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, c->ev0, c->ev1);
             c->last_ms = ms;                     // the attempt whose results are kept
@@ -254,62 +289,86 @@ static int run_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_
         const unsigned long long errS = st.err >> 8;
         if (code == E_TILE || code == E_EXTLIST) {
             if (c->tile_log2 > 12) { c->tile_log2--; continue; }
-            return set_err(c, PS4_ERR_CAP_REPS, "FATAL: tile capacity exceeded near S=%llu; this interval is NOT certified complete",
-                           errS);
+            static const char *list_name[5] = {"?", "selected-S list", "representation list", "4-set staging",
+                                               "extension list"};
+            return set_err(c, PS4_ERR_CAP_REPS,
+                           "FATAL: tile capacity exceeded near S=%llu (%s: %llu > %llu); this interval is NOT "
+                           "certified complete", errS, list_name[st.diag[0] < 5 ? st.diag[0] : 0], st.diag[1],
+                           st.diag[2]);
         }
         if (code != 0) {
             if (code == E_VERIFY)
-                return set_err(c, PS4_ERR_VERIFY, "BAD 4-set S=%llu [%lld,%lld,%lld,%lld]",
-                               st.verify_bad[0], (long long)st.verify_bad[1], (long long)st.verify_bad[2],
-                               (long long)st.verify_bad[3], (long long)st.verify_bad[4]);
+                return set_err(c, PS4_ERR_VERIFY, "BAD 4-set S=%llu [%lld,%lld,%lld,%lld]", st.verify_bad[0],
+                               (long long)st.verify_bad[1], (long long)st.verify_bad[2], (long long)st.verify_bad[3],
+                               (long long)st.verify_bad[4]);
             return set_err(c, (int)code, "FATAL: %s; this interval is NOT certified complete", fatal_text(code));
         }
         bool regrow = false;
-        if (st.n_hits > c->hits_cap) { if (grow32(c, c->d_hits, c->hits_cap, (uint64_t)st.n_hits * 3 / 2 + 1024)) return PS4_ERR_CUDA; regrow = true; }
-        if (st.n_exts > c->exts_cap) { if (grow32(c, c->d_exts, c->exts_cap, (uint64_t)st.n_exts * 3 / 2 + 1024)) return PS4_ERR_CUDA; regrow = true; }
-        if (st.n_sixes > c->sixes_cap) { if (grow32(c, c->d_sixes, c->sixes_cap, (uint64_t)st.n_sixes * 3 / 2 + 64)) return PS4_ERR_CUDA; regrow = true; }
+        if (st.n_hits > c->hits_cap) {
+            if (grow32(c, c->d_hits, c->hits_cap, (uint64_t)st.n_hits * 3 / 2 + 1024)) return PS4_ERR_CUDA;
+            regrow = true;
+        }
+        if (st.n_exts > c->exts_cap) {
+            if (grow32(c, c->d_exts, c->exts_cap, (uint64_t)st.n_exts * 3 / 2 + 1024)) return PS4_ERR_CUDA;
+            regrow = true;
+        }
+        if (st.n_sixes > c->sixes_cap) {
+            if (grow32(c, c->d_sixes, c->sixes_cap, (uint64_t)st.n_sixes * 3 / 2 + 64)) return PS4_ERR_CUDA;
+            regrow = true;
+        }
         if (regrow) continue;
-        // results are complete on the device
         if (res) {
-            res->n_quads = dump ? st.n_quads : 0;
-            if (dump && st.n_quads > res->quads_cap) {
+            res->n_quads = p.dump ? st.n_quads : 0;
+            if (p.dump && st.n_quads > res->quads_cap) {
                 res->n_hits = st.n_hits; res->n_exts = st.n_exts; res->n_sixes = st.n_sixes;
+                p.active = true;                 // results stay on the device: finish may be called again
                 return set_err(c, PS4_ERR_OUTPUT_FULL, "dump4 buffer holds %llu 4-sets, %llu needed",
                                (unsigned long long)res->quads_cap, st.n_quads);
             }
         }
-        // counters
         std::vector<unsigned long long> k((size_t)n_items * K_SLOTS);
         CUDA_TRY(c, cudaMemcpyAsync(k.data(), c->d_counters, k.size() * sizeof(unsigned long long),
                                     cudaMemcpyDeviceToHost, c->stream));
         std::vector<ps4_hit> hits(st.n_hits);
         std::vector<ps4_ext> exts(st.n_exts);
         std::vector<ps4_six> sixes(st.n_sixes);
-        if (st.n_hits) CUDA_TRY(c, cudaMemcpyAsync(hits.data(), c->d_hits, st.n_hits * sizeof(ps4_hit), cudaMemcpyDeviceToHost, c->stream));
-        if (st.n_exts) CUDA_TRY(c, cudaMemcpyAsync(exts.data(), c->d_exts, st.n_exts * sizeof(ps4_ext), cudaMemcpyDeviceToHost, c->stream));
-        if (st.n_sixes) CUDA_TRY(c, cudaMemcpyAsync(sixes.data(), c->d_sixes, st.n_sixes * sizeof(ps4_six), cudaMemcpyDeviceToHost, c->stream));
-        if (res && dump && st.n_quads)
-            CUDA_TRY(c, cudaMemcpyAsync(res->quads, c->d_quads, st.n_quads * sizeof(ps4_quad), cudaMemcpyDeviceToHost, c->stream));
+        if (st.n_hits)
+            CUDA_TRY(c, cudaMemcpyAsync(hits.data(), c->d_hits, st.n_hits * sizeof(ps4_hit), cudaMemcpyDeviceToHost,
+                                        c->stream));
+        if (st.n_exts)
+            CUDA_TRY(c, cudaMemcpyAsync(exts.data(), c->d_exts, st.n_exts * sizeof(ps4_ext), cudaMemcpyDeviceToHost,
+                                        c->stream));
+        if (st.n_sixes)
+            CUDA_TRY(c, cudaMemcpyAsync(sixes.data(), c->d_sixes, st.n_sixes * sizeof(ps4_six),
+                                        cudaMemcpyDeviceToHost, c->stream));
+        if (res && p.dump && st.n_quads)
+            CUDA_TRY(c, cudaMemcpyAsync(res->quads, c->d_quads, st.n_quads * sizeof(ps4_quad), cudaMemcpyDeviceToHost,
+                                        c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        c->d2h_bytes += k.size() * sizeof(unsigned long long) + st.n_hits * sizeof(ps4_hit) +
+                        st.n_exts * sizeof(ps4_ext) + st.n_sixes * sizeof(ps4_six) +
+                        ((res && p.dump) ? st.n_quads * sizeof(ps4_quad) : 0);
         if (res) {
             // deterministic order: item, S, then the reference's emission order (px, py, pz, class)
             std::vector<uint32_t> perm(hits.size());
             for (uint32_t i = 0; i < perm.size(); i++) perm[i] = i;
             std::sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
-                const ps4_hit &p = hits[x], &q = hits[y];
-                if (p.item != q.item) return p.item < q.item;
-                if (p.S != q.S) return p.S < q.S;
+                const ps4_hit &hp = hits[x], &hq = hits[y];
+                if (hp.item != hq.item) return hp.item < hq.item;
+                if (hp.S != hq.S) return hp.S < hq.S;
                 for (int i = 0; i < 4; i++)
-                    if (p.order[i] != q.order[i]) return p.order[i] < q.order[i];
+                    if (hp.order[i] != hq.order[i]) return hp.order[i] < hq.order[i];
                 return false;
             });
             res->n_hits = hits.size();
             res->n_exts = exts.size();
             res->n_sixes = sixes.size();
-            if (res->n_hits > res->hits_cap || res->n_exts > res->exts_cap || res->n_sixes > res->sixes_cap)
+            if (res->n_hits > res->hits_cap || res->n_exts > res->exts_cap || res->n_sixes > res->sixes_cap) {
+                p.active = true;                 // results stay on the device: finish may be called again
                 return set_err(c, PS4_ERR_OUTPUT_FULL, "result buffers too small: need hits=%llu exts=%llu sixes=%llu",
                                (unsigned long long)res->n_hits, (unsigned long long)res->n_exts,
                                (unsigned long long)res->n_sixes);
+            }
             std::vector<uint32_t> newpos(hits.size());
             uint32_t e = 0;
             for (uint32_t i = 0; i < perm.size(); i++) {
@@ -321,11 +380,11 @@ static int run_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_
                 res->hits[i] = h;
             }
             std::vector<ps4_six> sx = sixes;
-            for (auto &s : sx) s.hit = newpos[s.hit];
-            std::sort(sx.begin(), sx.end(), [](const ps4_six &p, const ps4_six &q) {
-                if (p.hit != q.hit) return p.hit < q.hit;
-                if (p.t != q.t) return p.t < q.t;
-                return p.s < q.s;
+            for (auto &s6 : sx) s6.hit = newpos[s6.hit];
+            std::sort(sx.begin(), sx.end(), [](const ps4_six &x, const ps4_six &y) {
+                if (x.hit != y.hit) return x.hit < y.hit;
+                if (x.t != y.t) return x.t < y.t;
+                return x.s < y.s;
             });
             for (size_t i = 0; i < sx.size(); i++) res->sixes[i] = sx[i];
         }
@@ -338,13 +397,35 @@ static int run_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_
 
 extern "C" int ps4_search_range(ps4_ctx *c, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res) {
     if (!c) return PS4_ERR_ARG;
-    if (lo < 1) lo = 1;
-    if (hi < lo) hi = lo;
-    return run_items(c, &lo, &hi, 1, stats, res);
+    int rc = begin_items(c, &lo, &hi, 1, res != nullptr, res ? res->quads_cap : 0);
+    if (rc == PS4_OK) rc = finish_items(c, stats, res);
+    c->pend.active = false;              // a synchronous call is repeated whole after any error
+    return rc;
 }
 
 extern "C" int ps4_search_batch(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, ps4_stats *stats,
                                 ps4_results *res) {
-    if (!c || !lo || !hi || n_items == 0) return set_err(c, PS4_ERR_ARG, "ps4_search_batch: empty batch");
-    return run_items(c, lo, hi, n_items, stats, res);
+    if (!c) return PS4_ERR_ARG;
+    if (!lo || !hi || n_items == 0) return set_err(c, PS4_ERR_ARG, "ps4_search_batch: empty batch");
+    int rc = begin_items(c, lo, hi, n_items, res != nullptr, res ? res->quads_cap : 0);
+    if (rc == PS4_OK) rc = finish_items(c, stats, res);
+    c->pend.active = false;
+    return rc;
+}
+
+extern "C" int ps4_search_enqueue(ps4_ctx *c, uint64_t lo, uint64_t hi) {
+    if (!c) return PS4_ERR_ARG;
+    int rc = begin_items(c, &lo, &hi, 1, false, 0);
+    if (rc) c->pend.active = false;
+    return rc;
+}
+
+extern "C" int ps4_search_finish(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
+    if (!c) return PS4_ERR_ARG;
+    return finish_items(c, stats, res);
+}
+
+extern "C" void ps4_last_transfer_bytes(const ps4_ctx *c, uint64_t *h2d, uint64_t *d2h) {
+    if (h2d) *h2d = c ? c->h2d_bytes : 0;
+    if (d2h) *d2h = c ? c->d2h_bytes : 0;
 }

@@ -42,6 +42,7 @@ struct Status {
     unsigned long long n_quads;
     unsigned int tile_next;        // persistent-kernel work counter
     unsigned int pad1;
+    unsigned long long diag[4];    // first internal-capacity event: which list, size, limit, S
 };
 
 // Arguments of one search launch (passed by value).
@@ -58,8 +59,8 @@ struct SearchArgs {
     ps4_ext *exts;   uint32_t exts_cap;
     ps4_six *sixes;  uint32_t sixes_cap;
     ps4_quad *quads; unsigned long long quads_cap;
-    uint32_t *scratch;         // per-CTA 4-set staging (batched kernel): 6 * quad_cap u32 per CTA
-    uint32_t quad_cap;         // 4-sets per tile the staging holds
+    uint32_t *scratch;         // per-CTA 4-set staging (batched kernel): 6 * stage_cap u32 per CTA
+    uint32_t stage_cap;        // 4-sets the staging of one CTA holds
     Status *status;
     uint32_t cap_reps, cap_divs, cap_ext;
     uint32_t flags;            // PS4_F_*
@@ -70,6 +71,6 @@ int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream);
 int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);
 size_t search_smem_bytes(int kernel, unsigned log2_tile);
 int search_block_threads();
-uint32_t quad_cap_for(unsigned log2_tile);
+uint32_t stage_cap_for(unsigned log2_tile, uint32_t cap_reps);
 
 }  // namespace ps4

@@ -188,6 +188,15 @@ __device__ __forceinline__ void raise_error(Status *st, unsigned code, uint64_t 
     atomicCAS(&st->err, 0ull, (ull)code | ((ull)S << 8));
 }
 
+// internal list overflow: record which list (1 = selected S, 2 = their representations,
+// 3 = staged 4-sets, 4 = tile extensions), its size and limit, then raise the re-run code
+__device__ __forceinline__ void raise_capacity(Status *st, unsigned code, unsigned which, uint64_t size,
+                                               uint64_t limit, uint64_t S) {
+    if (atomicCAS(&st->err, 0ull, (ull)code | ((ull)S << 8)) == 0ull) {
+        st->diag[0] = which; st->diag[1] = size; st->diag[2] = limit; st->diag[3] = S;
+    }
+}
+
 // Extend one 4-set (v, roots r) by every e: e+v_i square for all i.  Restates extend4
 // (s4.c:160-207) with the same difference choice (bi,bj,bk), the same counters and the
 // same order key (the reference's mixed-radix divisor index of the smaller divisor),
@@ -272,7 +281,7 @@ __device__ void extend_quad(const SearchArgs &a, const uint32_t r[6], const uint
                 for (int i = 0; i < 6; i++) x.r[i] = r[i];
                 x.lo = (uint64_t)e; x.hi = (uint64_t)(e >> 64);
             } else {
-                raise_error(a.status, E_EXTLIST, S);
+                raise_capacity(a.status, E_EXTLIST, 4, slot + 1, elist_cap, S);
             }
         }
         todd++;
@@ -334,6 +343,7 @@ struct TileShared {
     ull cnt[16];               // per-tile counters (K_* slots 0..12)
     uint32_t wsum[3 * NWARP];
     uint32_t n_is, n_rep, n_pairs, n_quads;
+    uint32_t n_staged, flushed;    // 4-sets staged for extension / already extended in this tile
     uint32_t elist_n, work;
     uint32_t binhist[NBIN], binstart[NBIN];
     uint32_t skip;             // tile abandoned (error)
@@ -352,8 +362,10 @@ struct TileLayout {
     static constexpr size_t OFF_IS_PBASE = OFF_IS_START + 2 * (size_t)IS_CAP;   // IS_CAP+1 u32 (pad to 8)
     static constexpr size_t OFF_REP_P = (OFF_IS_PBASE + 4 * ((size_t)IS_CAP + 2) + 15) & ~(size_t)15;
     static constexpr size_t OFF_REP_Q = OFF_REP_P + 4 * (size_t)REP_CAP;
-    static constexpr size_t BYTES = OFF_REP_Q + 4 * (size_t)REP_CAP;
-    static constexpr uint32_t ELIST_CAP = (uint32_t)((8 * (size_t)REP_CAP) / sizeof(ExtEntry));
+    static constexpr uint32_t ELIST_CAP = 256;                              // extensions per tile
+    static constexpr size_t OFF_ELIST = OFF_REP_Q + 4 * (size_t)REP_CAP;
+    static constexpr size_t BYTES = OFF_ELIST + ELIST_CAP * sizeof(ExtEntry);
+    static constexpr uint32_t FLUSH_AT = W / 2;                             // staged 4-sets that trigger P6
 };
 
 // locate a tile: tiles are handed out highest-S first (longest work first)
@@ -451,7 +463,10 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
         }
     }
     if (tot[0] > L::IS_CAP || tot[1] > L::REP_CAP) {
-        if (tid == 0) raise_error(a.status, E_TILE, S0);
+        if (tid == 0) {
+            if (tot[0] > L::IS_CAP) raise_capacity(a.status, E_TILE, 1, tot[0], L::IS_CAP, S0);
+            else raise_capacity(a.status, E_TILE, 2, tot[1], L::REP_CAP, S0);
+        }
         return false;
     }
     if (tid == 0) {
@@ -626,7 +641,9 @@ __device__ __forceinline__ void tile_flush_counters(const SearchArgs &a, TileSha
 __device__ __forceinline__ void tile_reset(TileShared &ts) {
     if (threadIdx.x < 16) ts.cnt[threadIdx.x] = 0;
     if (threadIdx.x < NBIN) ts.binhist[threadIdx.x] = 0;
-    if (threadIdx.x == 0) { ts.n_quads = 0; ts.elist_n = 0; ts.work = 0; ts.skip = 0; }
+    if (threadIdx.x == 0) {
+        ts.n_quads = 0; ts.n_staged = 0; ts.flushed = 0; ts.elist_n = 0; ts.work = 0; ts.skip = 0;
+    }
 }
 
 __device__ __forceinline__ void block_add_ext_counters(TileShared &ts, ull c, ull s, uint32_t md) {
@@ -649,13 +666,63 @@ __device__ __forceinline__ void decode_pair(uint32_t j, uint32_t &x, uint32_t &y
 
 // ================================================================== batched kernel
 
+// P5.5 + P6 over the staged 4-sets [0, staged): in chunks of up to W, order each chunk by
+// divisor-cost bin (most expensive first, so the longest walks start first), then warps pull
+// 32 staged 4-sets at a time and each lane extends one.
+template <int TL>
+__device__ void extend_staged(const SearchArgs &a, TileShared &ts, const uint32_t *scr, uint16_t *perm, ExtEntry *el,
+                              uint32_t staged, uint32_t qid_base, ull &c_cand, ull &c_sqrt, uint32_t &c_mdiv) {
+    using L = TileLayout<TL>;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t cap = a.stage_cap;
+    for (uint32_t c0 = 0; c0 < staged; c0 += L::W) {
+        const uint32_t c1 = min(c0 + L::W, staged), nc = c1 - c0;
+        if (tid < NBIN) ts.binhist[tid] = 0;
+        if (tid == 0) ts.work = 0;
+        __syncthreads();
+        for (uint32_t i = c0 + tid; i < c1; i += BS) atomicAdd(&ts.binhist[(scr[i] >> 22) & 15u], 1u);
+        __syncthreads();
+        if (tid == 0) {
+            uint32_t s = 0;
+            for (int b = NBIN - 1; b >= 0; b--) { ts.binstart[b] = s; s += ts.binhist[b]; }
+        }
+        __syncthreads();
+        for (uint32_t i = c0 + tid; i < c1; i += BS)
+            perm[atomicAdd(&ts.binstart[(scr[i] >> 22) & 15u], 1u)] = (uint16_t)(i - c0);
+        __syncthreads();
+        for (;;) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(&ts.work, 32u);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base >= nc) break;
+            const uint32_t pos = base + lane;
+            if (pos < nc) {
+                const uint32_t qi = c0 + perm[pos];
+                const uint32_t w0 = scr[qi];
+                uint32_t r[6];
+                r[0] = w0 & 0x3FFFFFu;
+                r[1] = scr[1 * cap + qi]; r[2] = scr[2 * cap + qi]; r[3] = scr[3 * cap + qi];
+                r[4] = scr[4 * cap + qi]; r[5] = scr[5 * cap + qi];
+                uint64_t v[4], S;
+                quad_values(r, v, S);
+                extend_quad(a, r, v, S, (w0 >> 26) & 3, (w0 >> 28) & 3, (w0 >> 30) & 3, qid_base + qi, c_cand,
+                            c_sqrt, c_mdiv, el, &ts.elist_n, L::ELIST_CAP);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <int TL>
 __global__ void __launch_bounds__(BS, 1) search_batched(const SearchArgs a) {
     using L = TileLayout<TL>;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ TileShared ts;
-    uint32_t *scr = a.scratch + (size_t)blockIdx.x * 6 * a.quad_cap;
-    const int tid = threadIdx.x, lane = tid & 31;
+    const uint32_t cap = a.stage_cap;
+    uint32_t *scr = a.scratch + (size_t)blockIdx.x * 6 * cap;
+    const int tid = threadIdx.x;
+    ExtEntry *el = (ExtEntry *)(smem + L::OFF_ELIST);
+    uint16_t *perm = (uint16_t *)(smem + L::OFF_CNT);           // the counters are dead after P3
 
     for (;;) {
         tile_reset(ts);
@@ -678,102 +745,79 @@ __global__ void __launch_bounds__(BS, 1) search_batched(const SearchArgs a) {
         const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
         const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
         const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
+        ull c_cand = 0, c_sqrt = 0;
+        uint32_t c_mdiv = 0;
 
-        // P5: 4-sets from every representation pair (x,y); only the z that give positive members
-        for (uint32_t gidx = tid; gidx < nPairs; gidx += BS) {
-            uint32_t lo = 0, hi = nI;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (is_pbase[mid] <= gidx) lo = mid; else hi = mid;
-            }
-            const uint32_t st = is_start[lo], k = is_k[lo];
-            const uint64_t S = S0 + is_off[lo];
-            uint32_t x, y;
-            decode_pair(gidx - is_pbase[lo], x, y);
-            const uint32_t px = rep_p[st + x], qx = rep_q[st + x], py = rep_p[st + y], qy = rep_q[st + y];
-            const uint64_t Px = (uint64_t)px * px, Py = (uint64_t)py * py;
-            const uint32_t pxy = (px + py) & 1;
-            const uint32_t Sodd = (uint32_t)(S & 1);
-            for (int cls = 0; cls < 2; cls++) {
-                // class 0: z upward while P_z < P_x + P_y;  class 1: z downward while P_z > S - P_x - P_y
-                const uint32_t want = cls == 0 ? 0u : Sodd;
-                for (uint32_t z = cls == 0 ? y + 1 : k - 1; z > y && z < k; z = cls == 0 ? z + 1 : z - 1) {
-                    const uint32_t pz = rep_p[st + z];
-                    const uint64_t Pz = (uint64_t)pz * pz;
-                    if (cls == 0 ? Pz >= Px + Py : Pz <= S - Px - Py) break;
-                    if (((pxy + pz) & 1) != want) continue;
-                    const uint32_t qz = rep_q[st + z];
-                    if (cls == 1 && qz == pz) continue;
-                    uint32_t r[6];
-                    r[0] = qx; r[1] = qy; r[4] = py; r[5] = px;
-                    r[2] = cls == 0 ? qz : pz;
-                    r[3] = cls == 0 ? pz : qz;
-                    uint64_t v[4], Sq;
-                    quad_values(r, v, Sq);
-                    if ((a.flags & PS4_F_VERIFY) && !quad_roots_ok(v, r)) { record_verify_failure(a, S, v); continue; }
-                    if (a.flags & PS4_F_DUMP4) dump_quad(a, r);
-                    const uint32_t qi = atomicAdd(&ts.n_quads, 1u);
-                    if (a.flags & PS4_F_NOEXT) continue;
-                    if (qi >= a.quad_cap) { raise_error(a.status, E_TILE, S0); continue; }
-                    int bi, bj, bk;
-                    uint32_t best;
-                    choose_pair(v, r, a.ndiv, bi, bj, bk, best);
-                    const uint32_t bin = min(31 - __clz(best | 1), NBIN - 1);
-                    atomicAdd(&ts.binhist[bin], 1u);
-                    scr[0 * a.quad_cap + qi] = r[0] | (bin << 22) | ((uint32_t)bi << 26) | ((uint32_t)bj << 28) |
-                                               ((uint32_t)bk << 30);
-                    scr[1 * a.quad_cap + qi] = r[1];
-                    scr[2 * a.quad_cap + qi] = r[2];
-                    scr[3 * a.quad_cap + qi] = r[3];
-                    scr[4 * a.quad_cap + qi] = r[4];
-                    scr[5 * a.quad_cap + qi] = r[5];
+        // P5 in waves of one representation pair (x,y) per thread; only the z that give positive
+        // members are visited.  A wave stages at most BS * 2(k-2) 4-sets, so the staging holds any
+        // wave on top of FLUSH_AT; whenever FLUSH_AT is passed (and after the last wave) the staged
+        // 4-sets are extended (P5.5/P6) and the staging restarts.
+        for (uint32_t wave = 0; wave < nPairs; wave += BS) {
+            const uint32_t gidx = wave + tid;
+            if (gidx < nPairs) {
+                uint32_t lo = 0, hi = nI;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (is_pbase[mid] <= gidx) lo = mid; else hi = mid;
                 }
+                const uint32_t st = is_start[lo], k = is_k[lo];
+                const uint64_t S = S0 + is_off[lo];
+                uint32_t x, y;
+                decode_pair(gidx - is_pbase[lo], x, y);
+                const uint32_t px = rep_p[st + x], qx = rep_q[st + x], py = rep_p[st + y], qy = rep_q[st + y];
+                const uint64_t Px = (uint64_t)px * px, Py = (uint64_t)py * py;
+                const uint32_t pxy = (px + py) & 1;
+                const uint32_t Sodd = (uint32_t)(S & 1);
+                for (int cls = 0; cls < 2; cls++) {
+                    // class 0: z upward while P_z < P_x + P_y;  class 1: z downward while P_z > S - P_x - P_y
+                    const uint32_t want = cls == 0 ? 0u : Sodd;
+                    for (uint32_t z = cls == 0 ? y + 1 : k - 1; z > y && z < k; z = cls == 0 ? z + 1 : z - 1) {
+                        const uint32_t pz = rep_p[st + z];
+                        const uint64_t Pz = (uint64_t)pz * pz;
+                        if (cls == 0 ? Pz >= Px + Py : Pz <= S - Px - Py) break;
+                        if (((pxy + pz) & 1) != want) continue;
+                        const uint32_t qz = rep_q[st + z];
+                        if (cls == 1 && qz == pz) continue;
+                        uint32_t r[6];
+                        r[0] = qx; r[1] = qy; r[4] = py; r[5] = px;
+                        r[2] = cls == 0 ? qz : pz;
+                        r[3] = cls == 0 ? pz : qz;
+                        uint64_t v[4], Sq;
+                        quad_values(r, v, Sq);
+                        if ((a.flags & PS4_F_VERIFY) && !quad_roots_ok(v, r)) { record_verify_failure(a, S, v); continue; }
+                        if (a.flags & PS4_F_DUMP4) dump_quad(a, r);
+                        atomicAdd(&ts.n_quads, 1u);
+                        if (a.flags & PS4_F_NOEXT) continue;
+                        const uint32_t si = atomicAdd(&ts.n_staged, 1u);
+                        if (si >= cap) { raise_capacity(a.status, E_TILE, 3, si + 1, cap, S0); continue; }
+                        int bi, bj, bk;
+                        uint32_t best;
+                        choose_pair(v, r, a.ndiv, bi, bj, bk, best);
+                        const uint32_t bin = min(31 - __clz(best | 1), NBIN - 1);
+                        scr[0 * cap + si] = r[0] | (bin << 22) | ((uint32_t)bi << 26) | ((uint32_t)bj << 28) |
+                                            ((uint32_t)bk << 30);
+                        scr[1 * cap + si] = r[1];
+                        scr[2 * cap + si] = r[2];
+                        scr[3 * cap + si] = r[3];
+                        scr[4 * cap + si] = r[4];
+                        scr[5 * cap + si] = r[5];
+                    }
+                }
+            }
+            __syncthreads();
+            const uint32_t staged = min(ts.n_staged, cap);
+            if (staged > 0 && (staged >= L::FLUSH_AT || wave + BS >= nPairs)) {      // block-uniform
+                extend_staged<TL>(a, ts, scr, perm, el, staged, ts.flushed, c_cand, c_sqrt, c_mdiv);
+                if (tid == 0) { ts.flushed += staged; ts.n_staged = 0; }
+                __syncthreads();
             }
         }
+        block_add_ext_counters(ts, c_cand, c_sqrt, c_mdiv);
         __syncthreads();
-        if (tid == 0) ts.cnt[K_SETS4] += ts.n_quads;
-        const uint32_t nq = min(ts.n_quads, a.quad_cap);
-        if (!(a.flags & PS4_F_NOEXT) && nq > 0) {
-            // P5.5: order the staged 4-sets by bin, most expensive first
-            uint16_t *perm = (uint16_t *)(smem + L::OFF_CNT);
-            if (tid == 0) {
-                uint32_t s = 0;
-                for (int b = NBIN - 1; b >= 0; b--) { ts.binstart[b] = s; s += ts.binhist[b]; }
-            }
-            __syncthreads();
-            for (uint32_t qi = tid; qi < nq; qi += BS) {
-                const uint32_t bin = (scr[qi] >> 22) & 15u;
-                perm[atomicAdd(&ts.binstart[bin], 1u)] = (uint16_t)qi;
-            }
-            __syncthreads();
-            // P6: extension, warps pull 32 staged 4-sets at a time
-            ExtEntry *el = (ExtEntry *)(smem + L::OFF_REP_P);
-            ull c_cand = 0, c_sqrt = 0;
-            uint32_t c_mdiv = 0;
-            for (;;) {
-                uint32_t base = 0;
-                if (lane == 0) base = atomicAdd(&ts.work, 32u);
-                base = __shfl_sync(0xffffffffu, base, 0);
-                if (base >= nq) break;
-                const uint32_t pos = base + lane;
-                if (pos < nq) {
-                    const uint32_t qi = perm[pos];
-                    const uint32_t w0 = scr[qi];
-                    uint32_t r[6];
-                    r[0] = w0 & 0x3FFFFFu;
-                    r[1] = scr[1 * a.quad_cap + qi]; r[2] = scr[2 * a.quad_cap + qi];
-                    r[3] = scr[3 * a.quad_cap + qi]; r[4] = scr[4 * a.quad_cap + qi];
-                    r[5] = scr[5 * a.quad_cap + qi];
-                    uint64_t v[4], S;
-                    quad_values(r, v, S);
-                    extend_quad(a, r, v, S, (w0 >> 26) & 3, (w0 >> 28) & 3, (w0 >> 30) & 3, qi, c_cand, c_sqrt,
-                                c_mdiv, el, &ts.elist_n, L::ELIST_CAP);
-                }
-            }
-            block_add_ext_counters(ts, c_cand, c_sqrt, c_mdiv);
-            __syncthreads();
-            // P7
-            if (tid == 0 && ts.elist_n) tile_report(a, ts, el, min(ts.elist_n, L::ELIST_CAP), item);
+        // P7
+        if (tid == 0) {
+            ts.cnt[K_SETS4] += ts.n_quads;
+            if (ts.elist_n) tile_report(a, ts, el, min(ts.elist_n, L::ELIST_CAP), item);
         }
         __syncthreads();
         tile_flush_counters(a, ts, item);
@@ -878,7 +922,11 @@ __global__ void build_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t n) {
 
 int search_block_threads() { return BS; }
 
-uint32_t quad_cap_for(unsigned log2_tile) { return 1u << log2_tile; }
+// staging per CTA: FLUSH_AT plus the most one P5 wave can stage, BS pairs x 2(k-2) 4-sets each
+uint32_t stage_cap_for(unsigned log2_tile, uint32_t cap_reps) {
+    const uint32_t k = cap_reps > 2 ? cap_reps : 3;
+    return (1u << log2_tile) / 2 + (uint32_t)BS * 2u * (k - 2u);
+}
 
 size_t search_smem_bytes(int kernel, unsigned log2_tile) {
     (void)kernel;

@@ -344,6 +344,7 @@ int main(int argc, char **argv) {
     }
     batch_out bo;
     memset(&bo, 0, sizeof bo);
+    if (opt_dump4) ensure((void **)&bo.r.quads, &bo.r.quads_cap, 1u << 16, sizeof(ps4_quad));
     double t0 = now_sec(), last_ckpt = -1e9;
     int last_report = 0;
     u64 chunks_per_batch = 1;

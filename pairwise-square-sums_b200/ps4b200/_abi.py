@@ -109,6 +109,9 @@ def load() -> C.CDLL:
         "ps4_search_range": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, P(Stats), P(Results)]),
         "ps4_search_batch": (C.c_int, [C.c_void_p, P(C.c_uint64), P(C.c_uint64), C.c_uint32, P(Stats),
                                        P(Results)]),
+        "ps4_search_enqueue": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
+        "ps4_search_finish": (C.c_int, [C.c_void_p, P(Stats), P(Results)]),
+        "ps4_last_transfer_bytes": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
         "ps4_format_hit": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),
         "ps4_format_six": (C.c_long, [P(Hit), P(Ext), P(Six), C.c_char_p, C.c_size_t]),
         "ps4_format_drill": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),

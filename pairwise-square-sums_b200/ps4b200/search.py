@@ -134,6 +134,26 @@ class Search:
             self._collect(out)
         return out
 
+    def enqueue(self, lo: int, hi: int) -> None:
+        """Start a search of [lo, hi) on the context's stream and return at once."""
+        rc = self.lib.ps4_search_enqueue(self.ctx, lo, hi)
+        if rc != _abi.PS4_OK:
+            raise Ps4Error(rc, self.lib.ps4_last_error(self.ctx).decode())
+
+    def finish(self, *, want_lines: bool = True) -> RangeResult:
+        """Wait for the enqueued search and collect it like ``range``."""
+        st = _abi.Stats()
+        self._call(lambda: self.lib.ps4_search_finish(self.ctx, C.byref(st), C.byref(self._res)))
+        out = RangeResult(stats=st.as_dict(), kernel_ms=self.last_kernel_ms)
+        if want_lines:
+            self._collect(out)
+        return out
+
+    def transfer_bytes(self) -> tuple[int, int]:
+        h2d, d2h = C.c_uint64(), C.c_uint64()
+        self.lib.ps4_last_transfer_bytes(self.ctx, C.byref(h2d), C.byref(d2h))
+        return int(h2d.value), int(d2h.value)
+
     def batch(self, los, his, *, want_lines: bool = True):
         """Many subranges in one launch: (per-item stats list, RangeResult with item tags)."""
         n = len(los)
