@@ -146,6 +146,27 @@ int ps4_search_finish(ps4_ctx *ctx, ps4_stats *stats, ps4_results *res);
 /* Bytes copied host->device and device->host by the last search call (inputs and results). */
 void ps4_last_transfer_bytes(const ps4_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 
+/* ps4_search_range without any device allocation.  No counterpart in the reference (its
+ * CPU engine allocates on the host freely); this serves callers that cannot call cudaMalloc
+ * at search time -- code that owns a fixed device-memory budget or its own pool and must not
+ * grow it, or a serving loop that cannot afford cudaMalloc/cudaFree, which block the host
+ * and (cudaFree) synchronise the device.
+ *
+ * Same inputs and outputs as ps4_search_range: S in [lo, hi) and the context's factor
+ * tables (built by ps4_create, read only here) in, counters (+=) and host result records
+ * out, with the records in device order (not sorted).  The only other device memory it
+ * uses is one static array in the library of 65.5 MB (62.5 MiB) -- 4-set staging for 148
+ * CTAs plus fixed result buffers of 65536 hits, 131072 extensions and 256 6-sets -- which
+ * every GPU that loads the library holds until the process exits.  It rejects, with
+ * PS4_ERR_ARG and a message, contexts made with PS4_F_DUMP4 or cap_reps > 512, ranges past
+ * the context's s_hi_max and ranges of 2^43 S or more; more records than the fixed buffers
+ * hold give PS4_ERR_OUTPUT_FULL (search a shorter range).  The first call on each device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that first call before
+ * any stream capture.  Every call on a device shares the array and overwrites it: calls whose
+ * work overlaps on the GPU (other threads, other streams) race and must be serialised by the
+ * caller.  Synchronous on the context's stream. */
+int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res);
+
 /* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
 double ps4_last_kernel_ms(const ps4_ctx *ctx);
 /* Number of kernel launches made by the last search call. */

@@ -429,3 +429,15 @@ extern "C" void ps4_last_transfer_bytes(const ps4_ctx *c, uint64_t *h2d, uint64_
     if (h2d) *h2d = c ? c->h2d_bytes : 0;
     if (d2h) *d2h = c ? c->d2h_bytes : 0;
 }
+
+// ---- read-only view of a context for the allocation-free entry point (ps4_kernels.cu) ----
+namespace ps4 {
+int ctx_view(ps4_ctx *c, CtxView *v) {
+    if (!c || !c->d_spfq) return PS4_ERR_ARG;
+    v->spfq = c->d_spfq; v->ndiv = c->d_ndiv; v->tab_n = c->tab_n; v->s_hi_max = c->cfg.s_hi_max;
+    v->cap_reps = c->cfg.cap_reps; v->cap_divs = c->cfg.cap_divs; v->cap_ext = c->cfg.cap_ext;
+    v->flags = c->cfg.flags; v->device = c->cfg.device; v->num_sms = c->num_sms; v->stream = c->stream;
+    return PS4_OK;
+}
+int ctx_fail(ps4_ctx *c, int code, const char *msg) { return set_err(c, code, "%s", msg); }
+}  // namespace ps4

@@ -66,6 +66,18 @@ struct SearchArgs {
     uint32_t flags;            // PS4_F_*
 };
 
+// Read-only view of a context (ps4_api.cu), for the allocation-free entry point.
+struct CtxView {
+    const uint64_t *spfq;
+    const uint16_t *ndiv;
+    uint64_t tab_n, s_hi_max;
+    uint32_t cap_reps, cap_divs, cap_ext, flags;
+    int device, num_sms;
+    void *stream;
+};
+int ctx_view(ps4_ctx *c, CtxView *v);
+int ctx_fail(ps4_ctx *c, int code, const char *msg);
+
 // Launchers (ps4_kernels.cu).  Return a cudaError_t value.
 int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream);
 int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);

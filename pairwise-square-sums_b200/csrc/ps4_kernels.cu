@@ -26,6 +26,10 @@
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
 
 #include "ps4_internal.h"
 
@@ -965,3 +969,279 @@ int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream) 
 }
 
 }  // namespace ps4
+
+// ================================================================== allocation-free variant
+//
+// ps4_search_range_noalloc (include/ps4.h) runs a variant of the batched kernel whose only
+// device memory beyond the context's read-only factor tables is one file-scope array,
+// ps4_noalloc_scratch below: the per-CTA 4-set staging plus small fixed result buffers.
+
+namespace ps4 {
+namespace noalloc {
+constexpr int TL = 12;                        // S values per tile: 4096
+constexpr uint32_t CTAS = 148;                // at most one CTA per SM of a B200
+constexpr uint32_t STAGE = 16384;             // staged 4-sets per CTA
+constexpr uint32_t HITS = 65536, EXTS = 131072, SIXES = 256;
+constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t OFF_STAGE = 0;
+constexpr size_t OFF_STATUS = al(OFF_STAGE + (size_t)CTAS * 6 * STAGE * sizeof(uint32_t));
+constexpr size_t OFF_COUNTERS = al(OFF_STATUS + sizeof(Status));
+constexpr size_t OFF_ITEM = al(OFF_COUNTERS + K_SLOTS * sizeof(unsigned long long));
+constexpr size_t OFF_HITS = al(OFF_ITEM + sizeof(Item));
+constexpr size_t OFF_EXTS = al(OFF_HITS + (size_t)HITS * sizeof(ps4_hit));
+constexpr size_t OFF_SIXES = al(OFF_EXTS + (size_t)EXTS * sizeof(ps4_ext));
+constexpr size_t BYTES = al(OFF_SIXES + (size_t)SIXES * sizeof(ps4_six));   // 65.5 MB (62.5 MiB)
+}  // namespace noalloc
+
+// The batched kernel with a fixed staging of STAGE 4-sets per CTA: the width of each P5 wave
+// (representation pairs emitted before the staging is checked) is set per tile from its
+// largest representation count k, so that one wave stages at most 2(k-2) 4-sets per pair
+// on top of FLUSH_AT and can never overflow the staging.  Otherwise as search_batched.
+template <int TL>
+__global__ void __launch_bounds__(BS, 1) search_batched_fixed(const SearchArgs a) {
+    using L = TileLayout<TL>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ TileShared ts;
+    const uint32_t cap = a.stage_cap;
+    uint32_t *scr = a.scratch + (size_t)blockIdx.x * 6 * cap;
+    const int tid = threadIdx.x;
+    ExtEntry *el = (ExtEntry *)(smem + L::OFF_ELIST);
+    uint16_t *perm = (uint16_t *)(smem + L::OFF_CNT);
+
+    for (;;) {
+        tile_reset(ts);
+        if (tid == 0) {
+            ts.tile = atomicAdd((unsigned int *)&a.status->tile_next, 1u);
+            ts.skip = *(volatile ull *)&a.status->err != 0ull;
+        }
+        __syncthreads();
+        const uint64_t tile = ts.tile;
+        if (tile >= a.n_tiles || ts.skip) break;
+        uint32_t item, n;
+        uint64_t S0;
+        tile_bounds(a, tile, TL, item, S0, n);
+        if (!tile_reps<TL>(a, ts, smem, S0, n)) { __syncthreads(); continue; }
+
+        const uint16_t *is_off = (const uint16_t *)(smem + L::OFF_IS_OFF);
+        const uint16_t *is_k = (const uint16_t *)(smem + L::OFF_IS_K);
+        const uint16_t *is_start = (const uint16_t *)(smem + L::OFF_IS_START);
+        const uint32_t *is_pbase = (const uint32_t *)(smem + L::OFF_IS_PBASE);
+        const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
+        const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
+        const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
+        const uint32_t kmax = (uint32_t)ts.cnt[K_MAX_REPS];
+        const uint32_t per_pair = 2u * (kmax > 2 ? kmax - 2 : 1);
+        const uint32_t wave_w = max(1u, min((uint32_t)BS, (cap - L::FLUSH_AT) / per_pair));
+        ull c_cand = 0, c_sqrt = 0;
+        uint32_t c_mdiv = 0;
+
+        for (uint32_t wave = 0; wave < nPairs; wave += wave_w) {
+            const uint32_t gidx = wave + tid;
+            if (tid < wave_w && gidx < nPairs) {
+                uint32_t lo = 0, hi = nI;
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (is_pbase[mid] <= gidx) lo = mid; else hi = mid;
+                }
+                const uint32_t st = is_start[lo], k = is_k[lo];
+                const uint64_t S = S0 + is_off[lo];
+                uint32_t x, y;
+                decode_pair(gidx - is_pbase[lo], x, y);
+                const uint32_t px = rep_p[st + x], qx = rep_q[st + x], py = rep_p[st + y], qy = rep_q[st + y];
+                const uint64_t Px = (uint64_t)px * px, Py = (uint64_t)py * py;
+                const uint32_t pxy = (px + py) & 1;
+                const uint32_t Sodd = (uint32_t)(S & 1);
+                for (int cls = 0; cls < 2; cls++) {
+                    const uint32_t want = cls == 0 ? 0u : Sodd;
+                    for (uint32_t z = cls == 0 ? y + 1 : k - 1; z > y && z < k; z = cls == 0 ? z + 1 : z - 1) {
+                        const uint32_t pz = rep_p[st + z];
+                        const uint64_t Pz = (uint64_t)pz * pz;
+                        if (cls == 0 ? Pz >= Px + Py : Pz <= S - Px - Py) break;
+                        if (((pxy + pz) & 1) != want) continue;
+                        const uint32_t qz = rep_q[st + z];
+                        if (cls == 1 && qz == pz) continue;
+                        uint32_t r[6];
+                        r[0] = qx; r[1] = qy; r[4] = py; r[5] = px;
+                        r[2] = cls == 0 ? qz : pz;
+                        r[3] = cls == 0 ? pz : qz;
+                        uint64_t v[4], Sq;
+                        quad_values(r, v, Sq);
+                        if ((a.flags & PS4_F_VERIFY) && !quad_roots_ok(v, r)) { record_verify_failure(a, S, v); continue; }
+                        atomicAdd(&ts.n_quads, 1u);
+                        if (a.flags & PS4_F_NOEXT) continue;
+                        const uint32_t si = atomicAdd(&ts.n_staged, 1u);
+                        if (si >= cap) { raise_capacity(a.status, E_TILE, 3, si + 1, cap, S0); continue; }
+                        int bi, bj, bk;
+                        uint32_t best;
+                        choose_pair(v, r, a.ndiv, bi, bj, bk, best);
+                        const uint32_t bin = min(31 - __clz(best | 1), NBIN - 1);
+                        scr[0 * cap + si] = r[0] | (bin << 22) | ((uint32_t)bi << 26) | ((uint32_t)bj << 28) |
+                                            ((uint32_t)bk << 30);
+                        scr[1 * cap + si] = r[1];
+                        scr[2 * cap + si] = r[2];
+                        scr[3 * cap + si] = r[3];
+                        scr[4 * cap + si] = r[4];
+                        scr[5 * cap + si] = r[5];
+                    }
+                }
+            }
+            __syncthreads();
+            const uint32_t staged = min(ts.n_staged, cap);
+            if (staged > 0 && (staged >= L::FLUSH_AT || wave + wave_w >= nPairs)) {
+                extend_staged<TL>(a, ts, scr, perm, el, staged, ts.flushed, c_cand, c_sqrt, c_mdiv);
+                if (tid == 0) { ts.flushed += staged; ts.n_staged = 0; }
+                __syncthreads();
+            }
+        }
+        block_add_ext_counters(ts, c_cand, c_sqrt, c_mdiv);
+        __syncthreads();
+        if (tid == 0) {
+            ts.cnt[K_SETS4] += ts.n_quads;
+            if (ts.elist_n) tile_report(a, ts, el, min(ts.elist_n, L::ELIST_CAP), item);
+        }
+        __syncthreads();
+        tile_flush_counters(a, ts, item);
+        __syncthreads();
+    }
+}
+}  // namespace ps4
+
+// The whole device memory of ps4_search_range_noalloc beyond the caller's context: loaded
+// with the library's device code on every GPU that runs it, held until the process exits.
+static __device__ __align__(256) unsigned char ps4_noalloc_scratch[ps4::noalloc::BYTES];
+
+extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res) {
+    using namespace ps4;
+    namespace na = ps4::noalloc;
+    CtxView v;
+    if (ctx_view(ctx, &v) != PS4_OK) return PS4_ERR_ARG;
+    if (!stats || !res) return ctx_fail(ctx, PS4_ERR_ARG, "ps4_search_range_noalloc: stats and res are required");
+    if (v.flags & PS4_F_DUMP4)
+        return ctx_fail(ctx, PS4_ERR_ARG, "ps4_search_range_noalloc: --dump4 output has no fixed bound; use ps4_search_range");
+    if (v.cap_reps > 512)
+        return ctx_fail(ctx, PS4_ERR_ARG, "ps4_search_range_noalloc: its fixed 4-set staging supports cap_reps <= 512");
+    if (lo < 1) lo = 1;
+    if (hi < lo) hi = lo;
+    if (hi > v.s_hi_max)
+        return ctx_fail(ctx, PS4_ERR_ARG, "ps4_search_range_noalloc: S_hi exceeds the context's s_hi_max");
+    const uint64_t n_tiles = (hi - lo + (1ull << na::TL) - 1) >> na::TL;
+    if (n_tiles >= (1ull << 31))
+        return ctx_fail(ctx, PS4_ERR_ARG, "ps4_search_range_noalloc: range too large for one call; split it");
+    res->n_hits = res->n_exts = res->n_sixes = res->n_quads = 0;
+    if (n_tiles == 0) return PS4_OK;
+
+    // Once per device, with that device current: the device address of the static array.
+    // (The host-side name ps4_noalloc_scratch is only a stand-in and must not reach a kernel.)
+    static void *base_of[64];
+    if (v.device < 0 || v.device >= 64) return ctx_fail(ctx, PS4_ERR_ARG, "device ordinal out of range");
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess) return ctx_fail(ctx, PS4_ERR_CUDA, "cudaGetDevice failed");
+    if (prev != v.device && cudaSetDevice(v.device) != cudaSuccess)
+        return ctx_fail(ctx, PS4_ERR_CUDA, "cudaSetDevice failed");
+    int rc = PS4_OK;
+    char msg[256];
+    do {
+        if (!base_of[v.device]) {
+            void *p = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&p, ps4_noalloc_scratch);
+            if (e != cudaSuccess) {
+                snprintf(msg, sizeof msg, "cudaGetSymbolAddress(ps4_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+                rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
+                break;
+            }
+            base_of[v.device] = p;
+        }
+        unsigned char *base = (unsigned char *)base_of[v.device];
+        Status *d_status = (Status *)(base + na::OFF_STATUS);
+        unsigned long long *d_counters = (unsigned long long *)(base + na::OFF_COUNTERS);
+        Item *d_item = (Item *)(base + na::OFF_ITEM);
+        cudaStream_t s = (cudaStream_t)v.stream;
+        Item it;
+        it.lo = lo; it.hi = hi; it.tile_base = 0;
+        SearchArgs a;
+        memset(&a, 0, sizeof a);
+        a.items = d_item; a.n_items = 1; a.n_tiles = n_tiles; a.log2_tile = na::TL;
+        a.spfq = v.spfq; a.ndiv = v.ndiv; a.tab_n = v.tab_n;
+        a.counters = d_counters;
+        a.hits = (ps4_hit *)(base + na::OFF_HITS); a.hits_cap = na::HITS;
+        a.exts = (ps4_ext *)(base + na::OFF_EXTS); a.exts_cap = na::EXTS;
+        a.sixes = (ps4_six *)(base + na::OFF_SIXES); a.sixes_cap = na::SIXES;
+        a.scratch = (uint32_t *)(base + na::OFF_STAGE); a.stage_cap = na::STAGE;
+        a.status = d_status;
+        a.cap_reps = v.cap_reps; a.cap_divs = v.cap_divs; a.cap_ext = v.cap_ext;
+        a.flags = v.flags & ~(uint32_t)PS4_F_DUMP4;
+        const unsigned grid = (unsigned)std::min<uint64_t>(std::min<uint64_t>(na::CTAS, (uint64_t)v.num_sms), n_tiles);
+        const size_t smem = TileLayout<na::TL>::BYTES;
+        // what must start at zero: the status (error word, record counts, tile counter) and the counters
+        cudaError_t e = cudaMemcpyAsync(d_item, &it, sizeof it, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_status, 0, sizeof(Status), s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_counters, 0, K_SLOTS * sizeof(unsigned long long), s);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(search_batched_fixed<na::TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e == cudaSuccess) {
+            search_batched_fixed<na::TL><<<grid, BS, smem, s>>>(a);
+            e = cudaGetLastError();
+        }
+        Status st;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&st, d_status, sizeof st, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            snprintf(msg, sizeof msg, "ps4_search_range_noalloc: %s", cudaGetErrorString(e));
+            rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
+            break;
+        }
+        const unsigned code = (unsigned)(st.err & 0xFF);
+        if (code == E_CAP_REPS || code == E_CAP_DIVS || code == E_CAP_EXT) {
+            const char *what = code == E_CAP_REPS ? "representation" : code == E_CAP_DIVS ? "divisor" : "extension";
+            snprintf(msg, sizeof msg, "FATAL: %s capacity exceeded; this interval is NOT certified complete", what);
+            rc = ctx_fail(ctx, (int)code, msg);
+            break;
+        }
+        if (code == E_VERIFY) {
+            snprintf(msg, sizeof msg, "BAD 4-set S=%llu [%lld,%lld,%lld,%lld]", st.verify_bad[0],
+                     (long long)st.verify_bad[1], (long long)st.verify_bad[2], (long long)st.verify_bad[3],
+                     (long long)st.verify_bad[4]);
+            rc = ctx_fail(ctx, PS4_ERR_VERIFY, msg);
+            break;
+        }
+        if (code != 0) {
+            snprintf(msg, sizeof msg, "ps4_search_range_noalloc: a tile near S=%llu outgrew the fixed shared-memory "
+                     "lists; search it with ps4_search_range", st.err >> 8);
+            rc = ctx_fail(ctx, PS4_ERR_CAP_REPS, msg);
+            break;
+        }
+        if (st.n_hits > na::HITS || st.n_exts > na::EXTS || st.n_sixes > na::SIXES) {
+            snprintf(msg, sizeof msg, "ps4_search_range_noalloc: %u result records exceed the fixed buffers "
+                     "(%u hits); search a shorter range", st.n_hits, na::HITS);
+            rc = ctx_fail(ctx, PS4_ERR_OUTPUT_FULL, msg);
+            break;
+        }
+        res->n_hits = st.n_hits; res->n_exts = st.n_exts; res->n_sixes = st.n_sixes;
+        if (res->n_hits > res->hits_cap || res->n_exts > res->exts_cap || res->n_sixes > res->sixes_cap) {
+            rc = ctx_fail(ctx, PS4_ERR_OUTPUT_FULL, "ps4_search_range_noalloc: result buffers too small; n_* hold the sizes");
+            break;
+        }
+        unsigned long long k[K_SLOTS];
+        e = cudaMemcpyAsync(k, d_counters, sizeof k, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && st.n_hits)
+            e = cudaMemcpyAsync(res->hits, a.hits, st.n_hits * sizeof(ps4_hit), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && st.n_exts)
+            e = cudaMemcpyAsync(res->exts, a.exts, st.n_exts * sizeof(ps4_ext), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && st.n_sixes)
+            e = cudaMemcpyAsync(res->sixes, a.sixes, st.n_sixes * sizeof(ps4_six), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) {
+            snprintf(msg, sizeof msg, "ps4_search_range_noalloc: %s", cudaGetErrorString(e));
+            rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
+            break;
+        }
+        uint64_t *add = &stats->S_done;
+        for (int i = 0; i < 10; i++) add[i] += k[i];
+        for (int i = 0; i < 100; i++) stats->hist5[i] += k[K_HIST5 + i];
+        stats->max_reps = std::max<uint64_t>(stats->max_reps, k[K_MAX_REPS]);
+        stats->max_divisors = std::max<uint64_t>(stats->max_divisors, k[K_MAX_DIVS]);
+        stats->max_extensions = std::max<uint64_t>(stats->max_extensions, k[K_MAX_EXT]);
+    } while (0);
+    if (prev != v.device) cudaSetDevice(prev);
+    return rc;
+}

@@ -109,6 +109,7 @@ def load() -> C.CDLL:
         "ps4_search_range": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, P(Stats), P(Results)]),
         "ps4_search_batch": (C.c_int, [C.c_void_p, P(C.c_uint64), P(C.c_uint64), C.c_uint32, P(Stats),
                                        P(Results)]),
+        "ps4_search_range_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, P(Stats), P(Results)]),
         "ps4_search_enqueue": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
         "ps4_search_finish": (C.c_int, [C.c_void_p, P(Stats), P(Results)]),
         "ps4_last_transfer_bytes": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
