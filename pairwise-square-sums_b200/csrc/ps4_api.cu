@@ -252,6 +252,7 @@ static int begin_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint3
         if (b < a) b = a;
         p.items[i].lo = a;
         p.items[i].hi = b;
+        p.items[i].id = i;
     }
     if (grow32(c, c->d_items, c->items_cap, n_items)) return PS4_ERR_CUDA;
     if (grow32(c, c->d_counters, c->counters_items, (uint64_t)n_items * K_SLOTS)) return PS4_ERR_CUDA;

@@ -25,13 +25,17 @@ enum {
     E_CAP_EXT = PS4_ERR_CAP_EXT,
     E_VERIFY = PS4_ERR_VERIFY,
     E_TILE = 100,      // a tile outgrew its shared-memory lists: re-run with smaller tiles
-    E_EXTLIST = 101    // more extensions in one tile than the per-tile list holds: re-run smaller
+    E_EXTLIST = 101,   // more extensions in one tile than the per-tile list holds: re-run smaller
+    E_QUEUE = 102      // the 4-set job queue of a batch overflowed: re-run with narrower batches
 };
 
-// One query item: every S in [lo, hi).  Tiles of the item are numbered from tile_base.
+// One query segment: every S in [lo, hi) of query item `id`.  Tiles of the segment are
+// numbered from tile_base.
 struct Item {
     uint64_t lo, hi;
-    uint64_t tile_base;   // prefix sum of tile counts over the items before this one
+    uint64_t tile_base;   // prefix sum of tile counts over the segments before this one
+    uint32_t id;          // the query item the segment belongs to (counters, hit records)
+    uint32_t pad;
 };
 
 // Status block copied back after every launch.
@@ -40,9 +44,11 @@ struct Status {
     unsigned long long verify_bad[5];  // --verify failure: S, a, b, c, d
     unsigned int n_hits, n_exts, n_sixes, pad0;
     unsigned long long n_quads;
-    unsigned int tile_next;        // persistent-kernel work counter
-    unsigned int pad1;
     unsigned long long diag[4];    // first internal-capacity event: which list, size, limit, S
+    // per batch of the two-kernel pipeline (cleared before every batch)
+    unsigned long long n_jobs;     // 4-sets queued by gen_jobs
+    unsigned int tile_next;        // tile work counter of the tile kernels
+    unsigned int ext_next;         // extend_jobs work counter (warp batches handed out)
 };
 
 // Arguments of one search launch (passed by value).
@@ -64,6 +70,8 @@ struct SearchArgs {
     Status *status;
     uint32_t cap_reps, cap_divs, cap_ext;
     uint32_t flags;            // PS4_F_*
+    uint32_t *jobs;            // 4-set job queue between gen_jobs and extend_jobs: 6 * jobs_cap u32 (SoA)
+    uint64_t jobs_cap;
 };
 
 // Read-only view of a context (ps4_api.cu), for the allocation-free entry point.
@@ -80,6 +88,11 @@ int ctx_fail(ps4_ctx *c, int code, const char *msg);
 
 // Launchers (ps4_kernels.cu).  Return a cudaError_t value.
 int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream);
+// two-kernel pipeline (ps4_extend.cu): 4-set generation into the job queue, then extension
+int launch_gen(const SearchArgs &a, int grid, void *stream);
+int launch_ext(const SearchArgs &a, int grid, void *stream);
+int gen_grid(int num_sms);
+int ext_grid(int num_sms);
 int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);
 size_t search_smem_bytes(int kernel, unsigned log2_tile);
 int search_block_threads();
