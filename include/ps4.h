@@ -44,8 +44,10 @@ enum {
 
 /* ---- kernel choice (ps4_config.kernel) ---- */
 enum {
-    PS4_KERNEL_BATCHED = 0, /* persistent tile queue, cost-binned extension, compacted square tests */
-    PS4_KERNEL_PLAIN = 1    /* one CTA per tile, one thread per S, inline extension (baseline)       */
+    PS4_KERNEL_BATCHED = 0, /* per batch of S: persistent tile kernel queues every 4-set, then the
+                               extension engine pools their divisor pairs warp-wide (default)        */
+    PS4_KERNEL_PLAIN = 1,   /* one CTA per tile, one thread per S, inline extension (baseline)       */
+    PS4_KERNEL_FUSED = 2    /* one persistent kernel: tiles, staging and per-lane extension fused    */
 };
 
 typedef struct ps4_ctx ps4_ctx;

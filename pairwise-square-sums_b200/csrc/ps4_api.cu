@@ -49,6 +49,10 @@ struct ps4_ctx {
     uint64_t last_launches = 0;
     unsigned tile_log2 = 14;             // current tile size (may shrink on E_TILE)
     PendingSearch pend;
+    uint32_t *d_jobs = nullptr;          // 4-set job queue of the two-kernel pipeline (6 x jobs_cap u32)
+    uint64_t jobs_cap = 1ull << 27;
+    uint32_t batch_div = 1;              // narrows the batches after a queue overflow
+    bool fused_fallback = false;         // this call re-runs on the fused kernel (engine list overflow)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
     std::string err;
 };
@@ -108,7 +112,7 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     if (!c) return;
     cudaFree(c->d_spfq); cudaFree(c->d_ndiv); cudaFree(c->d_items); cudaFree(c->d_counters);
     cudaFree(c->d_hits); cudaFree(c->d_exts); cudaFree(c->d_sixes); cudaFree(c->d_quads);
-    cudaFree(c->d_scratch); cudaFree(c->d_status);
+    cudaFree(c->d_scratch); cudaFree(c->d_status); cudaFree(c->d_jobs);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -184,54 +188,129 @@ static const char *fatal_text(unsigned code) {
 
 // ---- one search = enqueue (host prep + launch, no wait) + finish (wait, check, collect) ----
 
+// 4-sets per S grow slowly with S (0.13 below 1e10, 0.29 near 2e12); a batch of the
+// two-kernel pipeline is sized so that this bound, with margin, fills at most 90 % of the queue.
+static double jobs_per_S_bound(uint64_t S_hi) {
+    const double dec = S_hi > 1000000000ull ? std::log10((double)S_hi / 1e9) : 0.0;
+    return 0.25 + 0.05 * dec;
+}
+
 static int enqueue_items(ps4_ctx *c) {
     PendingSearch &p = c->pend;
     const uint32_t n_items = (uint32_t)p.items.size();
     const unsigned TL = c->tile_log2;
-    uint64_t tiles_total = 0;
-    for (uint32_t i = 0; i < n_items; i++) {
-        p.items[i].tile_base = tiles_total;
-        tiles_total += (p.items[i].hi - p.items[i].lo + (1ull << TL) - 1) >> TL;
-    }
-    if (tiles_total >= (1ull << 31))
-        return set_err(c, PS4_ERR_ARG, "range too large for one call (%llu tiles); split it",
-                       (unsigned long long)tiles_total);
-    p.tiles = tiles_total;
-    const int kernel = (int)c->cfg.kernel;
-    const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
-    int ctas_per_sm = c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1;
-    int grid = c->num_sms * ctas_per_sm;
-    if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
+    const int kernel = c->fused_fallback ? (int)PS4_KERNEL_FUSED : (int)c->cfg.kernel;
+    std::vector<Item> segs;                      // all batches' segments, batch after batch
+    std::vector<size_t> batch_start;             // segs index where each batch begins
+    std::vector<uint64_t> batch_tiles;
     if (kernel == PS4_KERNEL_BATCHED) {
-        uint64_t cap = c->scratch_words;
-        if (grow(c, c->d_scratch, cap, (uint64_t)grid * 6 * stage_cap)) return PS4_ERR_CUDA;
-        c->scratch_words = cap;
+        // cut the items into batches of at most ~90 % of the job queue in expected 4-sets
+        size_t i = 0;
+        uint64_t pos = n_items ? p.items[0].lo : 0;
+        while (i < n_items) {
+            batch_start.push_back(segs.size());
+            double budget = 0.9 * (double)c->jobs_cap / (double)c->batch_div;
+            uint64_t tiles = 0;
+            while (i < n_items && budget > 0) {
+                const Item &it = p.items[i];
+                if (pos < it.lo) pos = it.lo;
+                const double dens = jobs_per_S_bound(it.hi);
+                uint64_t room = (uint64_t)(budget / dens);
+                room = std::max<uint64_t>(room >> TL, 1) << TL;          // whole tiles
+                const uint64_t end = it.hi - pos > room ? pos + room : it.hi;
+                if (end > pos) {
+                    Item sg;
+                    sg.lo = pos; sg.hi = end; sg.id = it.id; sg.pad = 0;
+                    sg.tile_base = tiles;
+                    tiles += (end - pos + (1ull << TL) - 1) >> TL;
+                    segs.push_back(sg);
+                }
+                budget -= dens * (double)(end - pos);
+                pos = end;
+                if (pos >= it.hi) { i++; if (i < n_items) pos = p.items[i].lo; }
+            }
+            if (segs.size() == batch_start.back()) batch_start.pop_back();
+            else batch_tiles.push_back(tiles);
+        }
+    } else {
+        uint64_t tiles = 0;
+        for (uint32_t i = 0; i < n_items; i++) {
+            Item sg = p.items[i];
+            sg.tile_base = tiles;
+            tiles += (sg.hi - sg.lo + (1ull << TL) - 1) >> TL;
+            segs.push_back(sg);
+        }
+        batch_start.push_back(0);
+        batch_tiles.push_back(tiles);
     }
-    CUDA_TRY(c, cudaMemcpyAsync(c->d_items, p.items.data(), n_items * sizeof(Item), cudaMemcpyHostToDevice,
-                                c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long),
-                                c->stream));
+    uint64_t tiles_total = 0;
+    for (uint64_t t : batch_tiles) {
+        if (t >= (1ull << 31))
+            return set_err(c, PS4_ERR_ARG, "range too large for one call (%llu tiles); split it", (unsigned long long)t);
+        tiles_total += t;
+    }
+    p.tiles = tiles_total;
+    if (grow32(c, c->d_items, c->items_cap, std::max<size_t>(segs.size(), 1))) return PS4_ERR_CUDA;
+    if (!segs.empty())
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_items, segs.data(), segs.size() * sizeof(Item), cudaMemcpyHostToDevice,
+                                    c->stream));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long), c->stream));
     CUDA_TRY(c, cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
-    c->h2d_bytes += n_items * sizeof(Item);
+    c->h2d_bytes += segs.size() * sizeof(Item);
     SearchArgs a;
     memset(&a, 0, sizeof a);
-    a.items = c->d_items; a.n_items = n_items; a.n_tiles = tiles_total; a.log2_tile = TL;
+    a.log2_tile = TL;
     a.spfq = c->d_spfq; a.ndiv = c->d_ndiv; a.tab_n = c->tab_n;
     a.counters = c->d_counters;
     a.hits = c->d_hits; a.hits_cap = c->hits_cap;
     a.exts = c->d_exts; a.exts_cap = c->exts_cap;
     a.sixes = c->d_sixes; a.sixes_cap = c->sixes_cap;
     a.quads = p.dump ? c->d_quads : nullptr; a.quads_cap = p.dump ? c->quads_cap : 0;
-    a.scratch = c->d_scratch; a.stage_cap = stage_cap;
     a.status = c->d_status;
     a.cap_reps = c->cfg.cap_reps; a.cap_divs = c->cfg.cap_divs; a.cap_ext = c->cfg.cap_ext;
     a.flags = c->cfg.flags & (p.dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
-    if (tiles_total > 0) {
-        CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-        CUDA_TRY(c, (cudaError_t)launch_search(a, kernel, grid, c->stream));
-        CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+    CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+    if (kernel == PS4_KERNEL_BATCHED) {
+        if (!c->d_jobs) {
+            uint64_t cap = 0;
+            if (grow(c, c->d_jobs, cap, 6 * c->jobs_cap)) return PS4_ERR_CUDA;
+        }
+        a.jobs = c->d_jobs;
+        a.jobs_cap = c->jobs_cap;
+        const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
+        for (size_t b = 0; b < batch_start.size(); b++) {
+            const size_t s0 = batch_start[b], s1 = b + 1 < batch_start.size() ? batch_start[b + 1] : segs.size();
+            a.items = c->d_items + s0;
+            a.n_items = (uint32_t)(s1 - s0);
+            a.n_tiles = batch_tiles[b];
+            const int g = (int)std::min<uint64_t>((uint64_t)gen_grid(c->num_sms), std::max<uint64_t>(a.n_tiles, 1));
+            // n_jobs, tile_next, ext_next: the per-batch tail of the status block
+            CUDA_TRY(c, cudaMemsetAsync(&c->d_status->n_jobs, 0, 2 * sizeof(unsigned long long), c->stream));
+            CUDA_TRY(c, (cudaError_t)launch_gen(a, g, c->stream));
+            c->last_launches++;
+            if (ext) {
+                CUDA_TRY(c, (cudaError_t)launch_ext(a, ext_grid(c->num_sms), c->stream));
+                c->last_launches++;
+            }
+        }
+    } else if (tiles_total > 0) {
+        const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
+        int ctas_per_sm = c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1;
+        int grid = c->num_sms * ctas_per_sm;
+        if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
+        if (kernel == PS4_KERNEL_FUSED) {
+            uint64_t cap = c->scratch_words;
+            if (grow(c, c->d_scratch, cap, (uint64_t)grid * 6 * stage_cap)) return PS4_ERR_CUDA;
+            c->scratch_words = cap;
+        }
+        a.items = c->d_items; a.n_items = (uint32_t)segs.size(); a.n_tiles = tiles_total;
+        a.scratch = c->d_scratch; a.stage_cap = stage_cap;
+        // launch_search's selector: PS4_KERNEL_BATCHED there is the fused persistent kernel
+        CUDA_TRY(c, (cudaError_t)launch_search(a, kernel == PS4_KERNEL_PLAIN ? PS4_KERNEL_PLAIN : PS4_KERNEL_BATCHED,
+                                               grid, c->stream));
         c->last_launches++;
     }
+    CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
     return PS4_OK;
 }
@@ -241,6 +320,7 @@ static int begin_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint3
     if (c->pend.active) return set_err(c, PS4_ERR_ARG, "a search is already enqueued on this context");
     PendingSearch &p = c->pend;
     p.items.assign(n_items, Item{});
+    c->fused_fallback = false;
     c->last_launches = 0;
     c->last_ms = 0.0;
     c->h2d_bytes = c->d2h_bytes = 0;
@@ -288,6 +368,14 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
         const Status &st = *c->h_status;
         const unsigned code = (unsigned)(st.err & 0xFF);
         const unsigned long long errS = st.err >> 8;
+        if (code == E_QUEUE) {                   // a batch outgrew the job queue: narrower batches
+            if (c->batch_div < (1u << 16)) { c->batch_div *= 2; continue; }
+            return set_err(c, PS4_ERR_CUDA, "job queue overflow persists near S=%llu", errS);
+        }
+        if (code == E_EXTLIST && c->cfg.kernel == PS4_KERNEL_BATCHED && !c->fused_fallback) {
+            c->fused_fallback = true;            // > 16 extensions in one engine warp batch: fused kernel
+            continue;
+        }
         if (code == E_TILE || code == E_EXTLIST) {
             if (c->tile_log2 > 12) { c->tile_log2--; continue; }
             static const char *list_name[5] = {"?", "selected-S list", "representation list", "4-set staging",

@@ -1,0 +1,604 @@
+// ps4_extend.cu -- the batched search as two persistent kernels per batch of S:
+//
+//   gen_jobs<TL>  tiles of 2^TL S in shared memory (phases P1-P4 of ps4_device.cuh), then every
+//                 4-set of the tile (P5: closed-form z ranges per representation pair) is
+//                 written to a global job queue: a count pass, one block scan, one atomic
+//                 reservation per tile, a write pass.                         (s4.c:280-341)
+//   extend_jobs   the extension engine.  A warp takes 32 queued 4-sets (one per lane).  Each
+//                 lane picks the difference to extend by, factors it and writes the odd part's
+//                 divisors, in the reference's mixed-radix order, into the warp's shared buffer.
+//                 Then the warp pools the candidates of all 32 4-sets -- the complementary
+//                 divisor pairs (f,g), f<g, of equal parity, each visited once -- and splits
+//                 them into 32 equal contiguous runs, one per lane, so every lane does the same
+//                 work whatever the divisor counts.  Residue filters mod 64/63/65 are bit tests
+//                 against per-4-set rotated residue masks; the candidates that pass (the
+//                 reference's ext_sqrt) go through a warp queue and are square-tested 32 at a
+//                 time.                                                        (s4.c:160-207)
+//
+// Every counter and every reported line is identical to the reference's.
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "ps4_device.cuh"
+
+namespace ps4 {
+
+// ================================================================== job records
+
+// A queued 4-set: its six pair roots (< 2^22) in six u32 arrays (SoA).  The query item id
+// (< 2^20) rides in the spare top bits of r_ac (bits 0..9 of the id) and r_ad (bits 10..19).
+__device__ __forceinline__ void put_job(uint32_t *jobs, uint64_t cap, uint64_t j, const uint32_t r[6],
+                                        uint32_t item) {
+    jobs[j] = r[0];
+    jobs[cap + j] = r[1] | ((item & 1023u) << 22);
+    jobs[2 * cap + j] = r[2] | (((item >> 10) & 1023u) << 22);
+    jobs[3 * cap + j] = r[3];
+    jobs[4 * cap + j] = r[4];
+    jobs[5 * cap + j] = r[5];
+}
+
+__device__ __forceinline__ void get_job(const uint32_t *jobs, uint64_t cap, uint64_t j, uint32_t r[6],
+                                        uint32_t &item) {
+    const uint32_t w1 = __ldg(&jobs[cap + j]), w2 = __ldg(&jobs[2 * cap + j]);
+    r[0] = __ldg(&jobs[j]);
+    r[1] = w1 & 0x3FFFFFu;
+    r[2] = w2 & 0x3FFFFFu;
+    r[3] = __ldg(&jobs[3 * cap + j]);
+    r[4] = __ldg(&jobs[4 * cap + j]);
+    r[5] = __ldg(&jobs[5 * cap + j]);
+    item = (w1 >> 22) | ((w2 >> 22) << 10);
+}
+
+// ================================================================== gen_jobs
+
+// The 4-sets of representation pair gidx of the tile (P5).  Counts them; with WRITE also
+// builds, checks, dumps and (when `store`) queues them at out, out+1, ...
+template <bool WRITE>
+__device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t gidx, uint32_t nI,
+                                               const uint16_t *is_off, const uint16_t *is_k,
+                                               const uint16_t *is_start, const uint32_t *is_pbase,
+                                               const uint32_t *rep_p, const uint32_t *rep_q, uint64_t S0,
+                                               uint32_t item, uint64_t out, bool store) {
+    uint32_t lo = 0, hi = nI;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (is_pbase[mid] <= gidx) lo = mid; else hi = mid;
+    }
+    const uint32_t st = is_start[lo], k = is_k[lo];
+    const uint64_t S = S0 + is_off[lo];
+    uint32_t x, y;
+    decode_pair(gidx - is_pbase[lo], x, y);
+    const uint32_t px = rep_p[st + x], py = rep_p[st + y];
+    const uint64_t Px = (uint64_t)px * px, Py = (uint64_t)py * py;
+    const uint32_t pxy = (px + py) & 1;
+    const uint32_t Sodd = (uint32_t)(S & 1);
+    uint32_t n = 0;
+    for (int cls = 0; cls < 2; cls++) {
+        // class 0: z upward while P_z < P_x + P_y;  class 1: z downward while P_z > S - P_x - P_y
+        const uint32_t want = cls == 0 ? 0u : Sodd;
+        for (uint32_t z = cls == 0 ? y + 1 : k - 1; z > y && z < k; z = cls == 0 ? z + 1 : z - 1) {
+            const uint32_t pz = rep_p[st + z];
+            const uint64_t Pz = (uint64_t)pz * pz;
+            if (cls == 0 ? Pz >= Px + Py : Pz <= S - Px - Py) break;
+            if (((pxy + pz) & 1) != want) continue;
+            const uint32_t qz = rep_q[st + z];
+            if (cls == 1 && qz == pz) continue;
+            if (WRITE) {
+                uint32_t r[6];
+                r[0] = rep_q[st + x]; r[1] = rep_q[st + y]; r[4] = py; r[5] = px;
+                r[2] = cls == 0 ? qz : pz;
+                r[3] = cls == 0 ? pz : qz;
+                if (a.flags & PS4_F_VERIFY) {
+                    uint64_t v[4], Sq;
+                    quad_values(r, v, Sq);
+                    if (!quad_roots_ok(v, r)) record_verify_failure(a, S, v);
+                }
+                if (a.flags & PS4_F_DUMP4) dump_quad(a, r);
+                if (store) put_job(a.jobs, a.jobs_cap, out + n, r, item);
+            }
+            n++;
+        }
+    }
+    return n;
+}
+
+template <int TL>
+__global__ void __launch_bounds__(BS, 1) gen_jobs(const SearchArgs a) {
+    using L = TileLayout<TL>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ TileShared ts;
+    __shared__ unsigned long long s_base;
+    __shared__ int s_store;
+    const int tid = threadIdx.x;
+    const bool noext = (a.flags & PS4_F_NOEXT) != 0;
+    const bool need_write_pass = !noext || (a.flags & (PS4_F_DUMP4 | PS4_F_VERIFY));
+    for (;;) {
+        tile_reset(ts);
+        if (tid == 0) {
+            ts.tile = atomicAdd(&a.status->tile_next, 1u);
+            ts.skip = *(volatile ull *)&a.status->err != 0ull;
+        }
+        __syncthreads();
+        if (ts.tile >= a.n_tiles || ts.skip) break;                      // block-uniform
+        uint32_t item, n;
+        uint64_t S0;
+        tile_bounds(a, ts.tile, TL, item, S0, n);
+        if (!tile_reps<TL>(a, ts, smem, S0, n)) { __syncthreads(); continue; }
+        const uint16_t *is_off = (const uint16_t *)(smem + L::OFF_IS_OFF);
+        const uint16_t *is_k = (const uint16_t *)(smem + L::OFF_IS_K);
+        const uint16_t *is_start = (const uint16_t *)(smem + L::OFF_IS_START);
+        const uint32_t *is_pbase = (const uint32_t *)(smem + L::OFF_IS_PBASE);
+        const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
+        const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
+        const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
+        // count pass, one reservation for the tile, write pass in the same order
+        uint32_t mine = 0;
+        for (uint32_t g = tid; g < nPairs; g += BS)
+            mine += pair_quads<false>(a, g, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item, 0, false);
+        uint32_t off, d1, d2, tot[3];
+        block_scan3(mine, 0u, 0u, off, d1, d2, tot, ts.wsum);
+        if (tid == 0) {
+            ts.cnt[K_SETS4] += tot[0];
+            s_base = 0;
+            s_store = 0;
+            if (!noext && tot[0]) {
+                s_base = atomicAdd(&a.status->n_jobs, (ull)tot[0]);
+                if (s_base + tot[0] <= a.jobs_cap) s_store = 1;
+                else raise_capacity(a.status, E_QUEUE, 5, s_base + tot[0], a.jobs_cap, S0);
+            }
+        }
+        __syncthreads();
+        if (need_write_pass) {
+            const bool store = s_store != 0;
+            uint64_t pos = s_base + off;
+            for (uint32_t g = tid; g < nPairs; g += BS)
+                pos += pair_quads<true>(a, g, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item, pos, store);
+        }
+        __syncthreads();
+        tile_flush_counters(a, ts, item);
+        __syncthreads();
+    }
+}
+
+// ================================================================== extend_jobs
+
+constexpr int EBS = 256;                 // threads per CTA
+constexpr int EWARPS = EBS / 32;
+constexpr int DCAP = 384;                // odd divisors per warp (u64)
+constexpr int QCAP = 64;                 // square-test queue per warp
+constexpr int EXCAP = 16;                // extensions per warp batch
+
+struct EJob {                            // one lane's 4-set, read by every lane in phase B
+    uint64_t A, C1, C2;                  // extend by D = A - B; the other two members C1, C2
+    uint64_t m64a, m64b, m63a, m63b, m65a, m65b;   // rotated residue masks (see below)
+    uint64_t uA, uS;                     // u <= uA: e <= 0;  u <= uS: e <= max(v)
+    uint32_t nd, ncand, item;
+    uint16_t base, ndo;
+    uint8_t E2, flags;                   // flags: 1 = D even, 2/4 = residue 64 passes mod 65 (C1/C2)
+};
+
+struct WarpArea {
+    uint64_t dbuf[DCAP];
+    EJob job[32];
+    uint32_t cstart[33];
+    uint32_t qk[QCAP];
+    uint64_t qu[QCAP];
+    uint8_t qj[QCAP];
+    ExtEntry ext[EXCAP];
+    uint32_t n_ext;
+};
+
+// Rotated residue masks: bit s of the result is QR_m[(s + a) mod m], so the test of
+// e + C = u^2 + (C - A) becomes one shift of the mask by u^2 mod m.
+__device__ __forceinline__ uint64_t rot64(uint64_t x, uint32_t a) { return a ? (x >> a) | (x << (64 - a)) : x; }
+__device__ __forceinline__ uint64_t rot63(uint64_t x, uint32_t a) {
+    const uint64_t M = (1ull << 63) - 1;
+    return a ? ((x >> a) | (x << (63 - a))) & M : x;
+}
+__device__ __forceinline__ void rot65(uint32_t a, uint64_t &lo, uint32_t &bit64) {
+    const u128 X = (u128)QR65 | ((u128)1 << 64);            // residue 64 = 8^2 is a square
+    const u128 M = ((u128)1 << 65) - 1;
+    const u128 Y = a ? ((X >> a) | (X << (65 - a))) & M : X;
+    lo = (uint64_t)Y;
+    bit64 = (uint32_t)(Y >> 64) & 1u;
+}
+
+__device__ __forceinline__ uint32_t smod(int64_t d, uint32_t m) {
+    const int64_t r = d % (int64_t)m;
+    return (uint32_t)(r < 0 ? r + m : r);
+}
+
+// One lane's counters for the item of the 4-set it is working on, added to that item's
+// counter block whenever the item changes (queries of a batch are separate items).
+struct LaneCounters {
+    uint32_t item = 0xFFFFFFFFu;
+    ull cand = 0, sqrt_ = 0;
+    uint32_t mdiv = 0;
+    __device__ __forceinline__ void flush(const SearchArgs &a) {
+        if (item != 0xFFFFFFFFu) {
+            ull *k = a.counters + (size_t)item * K_SLOTS;
+            if (cand) atomicAdd(&k[K_EXT_CAND], cand);
+            if (sqrt_) atomicAdd(&k[K_EXT_SQRT], sqrt_);
+            if (mdiv) atomicMax(&k[K_MAX_DIVS], (ull)mdiv);
+        }
+        cand = 0; sqrt_ = 0; mdiv = 0;
+    }
+    __device__ __forceinline__ void use(const SearchArgs &a, uint32_t it) {
+        if (it != item) { flush(a); item = it; }
+    }
+};
+
+// Report the extensions of one warp batch: group them per 4-set, emit hit / ext / six
+// records and the counters sets5 / multi / sets6 / hist5 / max_extensions (s4.c:243-277).
+static __device__ void report_warp_exts(const SearchArgs &a, ExtEntry *el, uint32_t n) {
+    for (uint32_t x = 1; x < n; x++) {
+        ExtEntry k = el[x];
+        uint32_t y = x;
+        while (y > 0 && (el[y - 1].qid > k.qid || (el[y - 1].qid == k.qid && el[y - 1].key > k.key))) {
+            el[y] = el[y - 1];
+            y--;
+        }
+        el[y] = k;
+    }
+    for (uint32_t g0 = 0; g0 < n;) {
+        uint32_t g1 = g0 + 1;
+        while (g1 < n && el[g1].qid == el[g0].qid) g1++;
+        const uint32_t ne = g1 - g0;
+        uint32_t roots[6], item;                              // the 4-set and its item, from the queue
+        get_job(a.jobs, a.jobs_cap, el[g0].qid, roots, item);
+        ull *cnt = a.counters + (size_t)item * K_SLOTS;
+        uint64_t v[4], S;
+        quad_values(roots, v, S);
+        if (ne > a.cap_ext) { raise_error(a.status, E_CAP_EXT, S); g0 = g1; continue; }
+        atomicMax(&cnt[K_MAX_EXT], (ull)ne);
+        uint64_t vmax = v[0];
+        for (int i = 1; i < 4; i++) vmax = v[i] > vmax ? v[i] : vmax;
+        bool prints = ne >= 2;
+        for (uint32_t t = 0; t < ne; t++) prints |= (el[g0 + t].hi != 0 || el[g0 + t].lo > vmax);
+        uint32_t hslot = 0, eslot = 0;
+        if (prints) {
+            hslot = atomicAdd(&a.status->n_hits, 1u);
+            eslot = atomicAdd(&a.status->n_exts, ne);
+        }
+        uint32_t hflags = 0;
+        if (ne >= 2) {
+            hflags |= PS4_HIT_MULTI;
+            atomicAdd(&cnt[K_MULTI], 1ull);
+            u128 x[6] = {v[0], v[1], v[2], v[3], ((u128)el[g0].hi << 64) | el[g0].lo,
+                         ((u128)el[g0 + 1].hi << 64) | el[g0 + 1].lo};
+            if (verify_set(x, 6)) hflags |= PS4_HIT_DRILL_OK;
+        }
+        for (uint32_t t = 0; t < ne; t++) {
+            const u128 e = ((u128)el[g0 + t].hi << 64) | el[g0 + t].lo;
+            uint32_t ef = 0;
+            if (e > vmax) {
+                ef |= PS4_EXT_FIVE;
+                atomicAdd(&cnt[K_SETS5], 1ull);
+                int lg = 0;
+                for (u128 z = e; z > 1; z >>= 1) lg++;
+                atomicAdd(&cnt[K_HIST5 + (lg > 99 ? 99 : lg)], 1ull);
+                u128 x[5] = {v[0], v[1], v[2], v[3], e};
+                if (verify_set(x, 5)) ef |= PS4_EXT_FIVE_OK;
+            }
+            if (prints && eslot + t < a.exts_cap) {
+                ps4_ext rec;
+                rec.lo = el[g0 + t].lo; rec.hi = el[g0 + t].hi; rec.key = el[g0 + t].key; rec.flags = ef;
+                a.exts[eslot + t] = rec;
+            }
+        }
+        for (uint32_t t = 0; t < ne; t++)
+            for (uint32_t s = t + 1; s < ne; s++) {
+                const u128 et = ((u128)el[g0 + t].hi << 64) | el[g0 + t].lo;
+                const u128 es = ((u128)el[g0 + s].hi << 64) | el[g0 + s].lo;
+                if (!is_square_exact(et + es)) continue;
+                atomicAdd(&cnt[K_SETS6], 1ull);
+                u128 x[6] = {v[0], v[1], v[2], v[3], et, es};
+                const uint32_t sslot = atomicAdd(&a.status->n_sixes, 1u);
+                if (sslot < a.sixes_cap) {
+                    ps4_six rec;
+                    rec.hit = hslot; rec.t = t; rec.s = s; rec.flags = verify_set(x, 6) ? 1u : 0u;
+                    a.sixes[sslot] = rec;
+                }
+            }
+        if (prints && hslot < a.hits_cap) {
+            ps4_hit h;
+            h.S = S;
+            for (int i = 0; i < 4; i++) h.v[i] = v[i];
+            h.n_ext = ne; h.first_ext = eslot; h.flags = hflags; h.item = item;
+            h.order[0] = roots[5]; h.order[1] = roots[4];
+            h.order[2] = roots[2] < roots[3] ? roots[2] : roots[3];
+            h.order[3] = roots[2] < roots[3] ? 1u : 0u;
+            a.hits[hslot] = h;
+        }
+        g0 = g1;
+    }
+}
+
+// Phase A state of one lane: its 4-set, the difference to extend by and its factorisation.
+struct LaneJob {
+    uint32_t r[6], item;
+    uint64_t v[4], S, A, C1, C2;
+    int bi, bj, bk;
+    uint32_t pr[MAXP];
+    uint8_t ex[MAXP];
+    int np;
+    bool has2;
+    int E2, j0;
+    uint32_t ndo, nd, ncand;
+};
+
+// Returns false if the 4-set's difference has more divisors than cap_divs (fatal).
+__device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJob &J) {
+    get_job(a.jobs, a.jobs_cap, j, J.r, J.item);
+    quad_values(J.r, J.v, J.S);
+    uint32_t best;
+    choose_pair(J.v, J.r, a.ndiv, J.bi, J.bj, J.bk, best);
+    const uint32_t ra = pick6(J.r, pair_slot(J.bi, J.bk)), rb = pick6(J.r, pair_slot(J.bj, J.bk));
+    J.A = pick4(J.v, J.bi);
+    int o1 = -1, o2 = -1;
+#pragma unroll
+    for (int t = 0; t < 4; t++)
+        if (t != J.bi && t != J.bj) { if (o1 < 0) o1 = t; else o2 = t; }
+    J.C1 = pick4(J.v, o1);
+    J.C2 = pick4(J.v, o2);
+    J.np = 0;
+    factor_merge(a.spfq, ra - rb, J.pr, J.ex, J.np);
+    factor_merge(a.spfq, ra + rb, J.pr, J.ex, J.np);
+    // D even => both factors even => 2 is the first prime and 4 | D
+    J.has2 = J.np > 0 && J.pr[0] == 2;
+    J.E2 = J.has2 ? J.ex[0] : 0;
+    J.j0 = J.has2 ? 1 : 0;
+    uint32_t ndo = 1;
+    for (int q = J.j0; q < J.np; q++) ndo *= (uint32_t)J.ex[q] + 1;
+    J.ndo = ndo;
+    const uint64_t nd = (uint64_t)ndo * (uint64_t)(J.E2 + 1);
+    J.nd = (uint32_t)nd;
+    // same-parity complementary pairs with f < g: the reference's ext_cand (s4.c:191)
+    J.ncand = J.has2 ? (uint32_t)(((uint64_t)(J.E2 - 1) * ndo) >> 1) : (uint32_t)(nd >> 1);
+    if (nd > a.cap_divs) { raise_error(a.status, E_CAP_DIVS, J.S); return false; }
+    return true;
+}
+
+// Square tests of queue entries [first, first+count), one per lane (s4.c:199-203).
+__device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, uint32_t first, uint32_t count,
+                                              uint64_t bbase, int lane) {
+    if ((uint32_t)lane < count) {
+        const uint32_t idx = first + lane;
+        const uint64_t u = w->qu[idx];
+        const uint32_t jl = w->qj[idx];
+        const EJob &J = w->job[jl];
+        const u128 e = (u128)u * u - J.A;
+        if (is_square_fast(e + J.C1) && is_square_fast(e + J.C2)) {
+            const uint32_t slot = atomicAdd(&w->n_ext, 1u);
+            if (slot < EXCAP) {
+                ExtEntry &x = w->ext[slot];
+                x.qid = (uint32_t)(bbase + jl);
+                x.key = w->qk[idx];
+                x.lo = (uint64_t)e;
+                x.hi = (uint64_t)(e >> 64);
+            } else {
+                raise_capacity(a.status, E_EXTLIST, 4, slot + 1, EXCAP, 0);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
+    extern __shared__ __align__(16) unsigned char esmem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpArea *w = (WarpArea *)(esmem + (size_t)wid * sizeof(WarpArea));
+    const unsigned FULL = 0xffffffffu;
+    const uint64_t njobs = min(*(volatile ull *)&a.status->n_jobs, (ull)a.jobs_cap);
+    const uint64_t nbatch = (njobs + 31) >> 5;
+    if (lane == 0) w->n_ext = 0;
+    __syncwarp();
+    LaneCounters cnt;
+
+    for (;;) {
+        uint32_t b = 0;
+        int stop = 0;
+        if (lane == 0) {
+            b = atomicAdd(&a.status->ext_next, 1u);
+            stop = *(volatile ull *)&a.status->err != 0ull;
+        }
+        b = __shfl_sync(FULL, b, 0);
+        stop = __shfl_sync(FULL, stop, 0);
+        if (b >= nbatch || stop) break;                                  // warp-uniform
+        const uint64_t bbase = (uint64_t)b << 5;
+        const uint64_t jidx = bbase + lane;
+
+        // ---- phase A: one 4-set per lane
+        LaneJob J;
+        bool pending = jidx < njobs && job_setup(a, jidx, J);
+        const bool big = pending && J.ndo > (uint32_t)DCAP;
+        if (pending) {
+            cnt.use(a, J.item);
+            if (J.nd > cnt.mdiv) cnt.mdiv = J.nd;
+            if (!big) cnt.cand += J.ncand;
+        }
+        if (big) {                       // rare: more odd divisors than the warp buffer holds
+            uint32_t md = 0;
+            extend_quad(a, J.r, J.v, J.S, J.bi, J.bj, J.bk, (uint32_t)jidx, cnt.cand, cnt.sqrt_, md, w->ext,
+                        &w->n_ext, EXCAP);
+            pending = false;
+        }
+        while (__any_sync(FULL, pending)) {
+            // place the divisor lists of as many pending lanes as fit, in lane order
+            const uint32_t want = pending ? J.ndo : 0;
+            uint32_t incl = want;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const uint32_t base = incl - want;
+            const bool fits = pending && incl <= (uint32_t)DCAP;
+            if (fits) {
+                // odd divisors in mixed-radix order over the odd primes: the reference's
+                // gen_divisors order (s4.c:149-156) restricted to the odd part
+                uint64_t *d = w->dbuf + base;
+                d[0] = 1;
+                uint32_t nn = 1;
+                for (int q = J.j0; q < J.np; q++) {
+                    const uint32_t cur = nn;
+                    uint64_t pk = 1;
+                    for (int e = 1; e <= J.ex[q]; e++) {
+                        pk *= J.pr[q];
+                        for (uint32_t i = 0; i < cur; i++) d[nn++] = d[i] * pk;
+                    }
+                }
+                EJob &E = w->job[lane];
+                E.A = J.A; E.C1 = J.C1; E.C2 = J.C2;
+                const int64_t dd1 = (int64_t)J.C1 - (int64_t)J.A, dd2 = (int64_t)J.C2 - (int64_t)J.A;
+                E.m64a = rot64(QR64, smod(dd1, 64)); E.m64b = rot64(QR64, smod(dd2, 64));
+                E.m63a = rot63(QR63, smod(dd1, 63)); E.m63b = rot63(QR63, smod(dd2, 63));
+                uint32_t h1, h2;
+                rot65(smod(dd1, 65), E.m65a, h1);
+                rot65(smod(dd2, 65), E.m65b, h2);
+                uint64_t vmax = J.v[0];
+                for (int i = 1; i < 4; i++) vmax = J.v[i] > vmax ? J.v[i] : vmax;
+                E.uA = isqrt64(J.A);
+                E.uS = isqrt64(J.A + vmax);
+                E.nd = J.nd; E.ncand = J.ncand; E.item = J.item;
+                E.base = (uint16_t)base; E.ndo = (uint16_t)J.ndo;
+                E.E2 = (uint8_t)J.E2;
+                E.flags = (uint8_t)((J.has2 ? 1 : 0) | (h1 << 1) | (h2 << 2));
+            }
+            // ---- phase B: the pooled candidates, 32 equal contiguous runs
+            const uint32_t nc = fits ? J.ncand : 0;
+            uint32_t ci = nc;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(FULL, ci, o);
+                if (lane >= o) ci += y;
+            }
+            w->cstart[lane] = ci - nc;
+            const uint32_t C = __shfl_sync(FULL, ci, 31);
+            if (lane == 31) w->cstart[32] = C;
+            __syncwarp();
+            const uint32_t g0 = (uint32_t)(((uint64_t)lane * C) >> 5);
+            const uint32_t g1 = (uint32_t)(((uint64_t)(lane + 1) * C) >> 5);
+            const uint32_t iters = (C + 31) >> 5;
+            uint32_t jl = 0;
+            {
+                uint32_t lo = 0, hi = 32;                 // last job with cstart <= g0
+                while (hi - lo > 1) {
+                    const uint32_t mid = (lo + hi) >> 1;
+                    if (w->cstart[mid] <= g0) lo = mid; else hi = mid;
+                }
+                jl = lo;
+            }
+            // the current job of this lane's run, in registers
+            uint64_t A = 0, m64a = 0, m64b = 0, m63a = 0, m63b = 0, m65a = 0, m65b = 0, uA = 0, uS = 0;
+            uint32_t nd = 0, ncand = 0, jbase = 0, ndo = 0, E2 = 0, flg = 0, R = 1;
+            uint32_t cc = 0, t_odd = 0, d2 = 0;
+            auto load_job = [&](uint32_t j, uint32_t cidx) {
+                const EJob &E = w->job[j];
+                A = E.A; m64a = E.m64a; m64b = E.m64b; m63a = E.m63a; m63b = E.m63b; m65a = E.m65a; m65b = E.m65b;
+                uA = E.uA; uS = E.uS; nd = E.nd; ncand = E.ncand; jbase = E.base; ndo = E.ndo; E2 = E.E2;
+                flg = E.flags;
+                cnt.use(a, E.item);
+                cc = cidx;
+                if (flg & 1) { R = E2 - 1; t_odd = cidx / R; d2 = 1 + cidx % R; }
+                else { R = 1; t_odd = cidx; d2 = 0; }
+            };
+            if (g0 < g1) load_job(jl, g0 - w->cstart[jl]);
+            uint32_t qn = 0;
+            for (uint32_t it = 0; it < iters; it++) {
+                bool pass = false;
+                uint64_t u = 0;
+                uint32_t key = 0, jcur = jl;               // the job of THIS candidate
+                if (it < g1 - g0) {
+                    // candidate (t_odd, d2): f = 2^d2 * fo, g = 2^(E2-d2) * go with fo*go = D_odd
+                    const uint64_t fo = w->dbuf[jbase + t_odd], go = w->dbuf[jbase + ndo - 1 - t_odd];
+                    uint64_t f = fo << d2, g = go << (E2 - d2);
+                    const uint32_t t = (flg & 1) ? d2 + (E2 + 1) * t_odd : t_odd;
+                    key = t;                                // mixed-radix index of the smaller divisor
+                    if (f > g) { const uint64_t s = f; f = g; g = s; key = nd - 1 - t; }
+                    u = (f + g) >> 1;
+                    // e + C = u^2 + (C - A): residues mod 64, 63, 65 (s4.c:192-194)
+                    const uint32_t w64 = (uint32_t)u & 63u, s64 = (w64 * w64) & 63u;
+                    const uint32_t rr = (uint32_t)(u >> 24) + ((uint32_t)u & 0xFFFFFFu);   // 2^24 = 1 mod 63 and mod 65
+                    const uint32_t w63 = rr % 63u, s63 = (w63 * w63) % 63u;
+                    const uint32_t w65 = rr % 65u, s65 = (w65 * w65) % 65u;
+                    const uint32_t b65a = s65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65a >> s65) & 1u;
+                    const uint32_t b65b = s65 == 64u ? (flg >> 2) & 1u : (uint32_t)(m65b >> s65) & 1u;
+                    pass = ((m64a >> s64) & (m64b >> s64) & (m63a >> s63) & (m63b >> s63) & 1u) && (b65a & b65b) &&
+                           u > uA;
+                    if (pass && u <= uS) {                  // e <= max(v): rule out e in v (s4.c:197)
+                        const uint64_t e = u * u - A;
+                        uint32_t jr[6], jit;
+                        get_job(a.jobs, a.jobs_cap, bbase + jcur, jr, jit);
+                        uint64_t v[4], Sq;
+                        quad_values(jr, v, Sq);
+                        if (e == v[0] || e == v[1] || e == v[2] || e == v[3]) pass = false;
+                    }
+                    if (pass) cnt.sqrt_++;
+                    // next candidate of this lane's run
+                    if (flg & 1) { if (++d2 > R) { d2 = 1; t_odd++; } }
+                    else t_odd++;
+                    if (++cc == ncand && it + 1 < g1 - g0) {
+                        do { jl++; } while (jl < 31 && w->cstart[jl + 1] == w->cstart[jl]);
+                        load_job(jl, 0);
+                    }
+                }
+                const unsigned m = __ballot_sync(FULL, pass);
+                if (pass) {
+                    const uint32_t pos = qn + __popc(m & ((1u << lane) - 1u));
+                    w->qu[pos] = u;
+                    w->qk[pos] = key;
+                    w->qj[pos] = (uint8_t)jcur;
+                }
+                qn += __popc(m);
+                __syncwarp();
+                if (qn >= 32) {
+                    process_queue(a, w, qn - 32, 32, bbase, lane);
+                    qn -= 32;
+                    __syncwarp();
+                }
+            }
+            if (qn) process_queue(a, w, 0, qn, bbase, lane);
+            __syncwarp();
+            pending = pending && !fits;
+        }
+        __syncwarp();
+        if (lane == 0 && w->n_ext) {
+            report_warp_exts(a, w->ext, min(w->n_ext, (uint32_t)EXCAP));
+            w->n_ext = 0;
+        }
+        __syncwarp();
+    }
+    cnt.flush(a);
+}
+
+// ================================================================== launchers
+
+int gen_grid(int num_sms) { return num_sms; }
+int ext_grid(int num_sms) { return num_sms * 3; }
+
+template <int TL>
+static int launch_gen_tl(const SearchArgs &a, int grid, cudaStream_t s) {
+    const size_t smem = TileLayout<TL>::BYTES;
+    cudaFuncSetAttribute(gen_jobs<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    gen_jobs<TL><<<grid, BS, smem, s>>>(a);
+    return (int)cudaGetLastError();
+}
+
+int launch_gen(const SearchArgs &a, int grid, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (a.log2_tile) {
+        case 12: return launch_gen_tl<12>(a, grid, s);
+        case 13: return launch_gen_tl<13>(a, grid, s);
+        default: return launch_gen_tl<14>(a, grid, s);
+    }
+}
+
+int launch_ext(const SearchArgs &a, int grid, void *stream) {
+    const size_t smem = EWARPS * sizeof(WarpArea);
+    cudaFuncSetAttribute(extend_jobs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    extend_jobs<<<grid, EBS, smem, (cudaStream_t)stream>>>(a);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace ps4

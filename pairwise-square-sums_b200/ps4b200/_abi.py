@@ -30,6 +30,7 @@ PS4_F_DUMP4 = 4
 
 PS4_KERNEL_BATCHED = 0
 PS4_KERNEL_PLAIN = 1
+PS4_KERNEL_FUSED = 2
 
 PS4_HIT_MULTI = 1
 PS4_HIT_DRILL_OK = 2
