@@ -50,7 +50,8 @@ struct ps4_ctx {
     unsigned tile_log2 = 14;             // current tile size (may shrink on E_TILE)
     PendingSearch pend;
     uint32_t *d_jobs = nullptr;          // 4-set job queue of the two-kernel pipeline (6 x jobs_cap u32)
-    uint64_t jobs_cap = 1ull << 27;
+    uint64_t jobs_cap = 1ull << 20;          // grows with the calls, up to 2^27 (3.2 GB)
+    uint64_t d_jobs_words = 0;
     uint32_t batch_div = 1;              // narrows the batches after a queue overflow
     bool fused_fallback = false;         // this call re-runs on the fused kernel (engine list overflow)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
@@ -200,6 +201,12 @@ static int enqueue_items(ps4_ctx *c) {
     const uint32_t n_items = (uint32_t)p.items.size();
     const unsigned TL = c->tile_log2;
     const int kernel = c->fused_fallback ? (int)PS4_KERNEL_FUSED : (int)c->cfg.kernel;
+    if (kernel == PS4_KERNEL_BATCHED) {          // queue: the call's expected 4-sets, 2^20 .. 2^27
+        double need = 0;
+        for (uint32_t i = 0; i < n_items; i++)
+            need += jobs_per_S_bound(p.items[i].hi) * (double)(p.items[i].hi - p.items[i].lo);
+        while (c->jobs_cap < (1ull << 27) && (double)c->jobs_cap * 0.9 < need) c->jobs_cap <<= 1;
+    }
     std::vector<Item> segs;                      // all batches' segments, batch after batch
     std::vector<size_t> batch_start;             // segs index where each batch begins
     std::vector<uint64_t> batch_tiles;
@@ -271,9 +278,8 @@ static int enqueue_items(ps4_ctx *c) {
     a.flags = c->cfg.flags & (p.dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
     if (kernel == PS4_KERNEL_BATCHED) {
-        if (!c->d_jobs) {
-            uint64_t cap = 0;
-            if (grow(c, c->d_jobs, cap, 6 * c->jobs_cap)) return PS4_ERR_CUDA;
+        if (c->d_jobs_words < 6 * c->jobs_cap) {
+            if (grow(c, c->d_jobs, c->d_jobs_words, 6 * c->jobs_cap)) return PS4_ERR_CUDA;
         }
         a.jobs = c->d_jobs;
         a.jobs_cap = c->jobs_cap;

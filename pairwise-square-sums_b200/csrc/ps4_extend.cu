@@ -165,24 +165,29 @@ __global__ void __launch_bounds__(BS, 1) gen_jobs(const SearchArgs a) {
 
 constexpr int EBS = 256;                 // threads per CTA
 constexpr int EWARPS = EBS / 32;
-constexpr int DCAP = 384;                // odd divisors per warp (u64)
+constexpr int DCAP = 384;                // divisor-list entries per warp (u64)
 constexpr int QCAP = 64;                 // square-test queue per warp
 constexpr int EXCAP = 16;                // extensions per warp batch
 
+// The odd part D_odd of a difference is kept factored: its odd primes are split into a low
+// group (the first primes of the reference's order) and a high group, with divisor lists
+// lo[0..L) and hi[0..H) in mixed-radix order.  The odd divisor with mixed-radix index
+// t = l + L*h is lo[l]*hi[h], and its complement (index ndo-1-t) is lo[L-1-l]*hi[H-1-h]:
+// L+H entries instead of ndo = L*H.
 struct EJob {                            // one lane's 4-set, read by every lane in phase B
     uint64_t A, C1, C2;                  // extend by D = A - B; the other two members C1, C2
-    uint64_t m64a, m64b, m63a, m63b, m65a, m65b;   // rotated residue masks (see below)
+    uint64_t m64, m63, m65;              // bit s: u^2 + (C - A) is a residue for both C (mod 64/63/65)
     uint64_t uA, uS;                     // u <= uA: e <= 0;  u <= uS: e <= max(v)
     uint32_t nd, ncand, item;
-    uint16_t base, ndo;
-    uint8_t E2, flags;                   // flags: 1 = D even, 2/4 = residue 64 passes mod 65 (C1/C2)
+    uint16_t base, L, H;                 // lo list at dbuf[base..base+L), hi list right after it
+    uint8_t E2, flags;                   // flags: 1 = D even, 2 = residue 64 passes mod 65
 };
 
 struct WarpArea {
     uint64_t dbuf[DCAP];
     EJob job[32];
     uint32_t cstart[33];
-    uint32_t qk[QCAP];
+    uint32_t qidx[QCAP];                 // candidate: l | h << 12 | d2 << 24
     uint64_t qu[QCAP];
     uint8_t qj[QCAP];
     ExtEntry ext[EXCAP];
@@ -204,9 +209,13 @@ __device__ __forceinline__ void rot65(uint32_t a, uint64_t &lo, uint32_t &bit64)
     bit64 = (uint32_t)(Y >> 64) & 1u;
 }
 
-__device__ __forceinline__ uint32_t smod(int64_t d, uint32_t m) {
-    const int64_t r = d % (int64_t)m;
-    return (uint32_t)(r < 0 ? r + m : r);
+// (d mod 63, d mod 65) for |d| < 2^48, by folding 24-bit halves (2^24 = 1 mod 63 and mod 65)
+__device__ __forceinline__ void res6365(int64_t d, uint32_t &r63, uint32_t &r65) {
+    const uint64_t x = d < 0 ? (uint64_t)(-d) : (uint64_t)d;
+    const uint32_t r = (uint32_t)(x >> 24) + (uint32_t)(x & 0xFFFFFFu);
+    r63 = r % 63u;
+    r65 = r % 65u;
+    if (d < 0) { r63 = r63 ? 63u - r63 : 0u; r65 = r65 ? 65u - r65 : 0u; }
 }
 
 // One lane's counters for the item of the 4-set it is working on, added to that item's
@@ -324,8 +333,8 @@ struct LaneJob {
     uint8_t ex[MAXP];
     int np;
     bool has2;
-    int E2, j0;
-    uint32_t ndo, nd, ncand;
+    int E2, j0, js;                      // odd primes are pr[j0..np); the high group starts at js
+    uint32_t ndo, nd, ncand, L, H;
 };
 
 // Returns false if the 4-set's difference has more divisors than cap_divs (fatal).
@@ -352,6 +361,12 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
     uint32_t ndo = 1;
     for (int q = J.j0; q < J.np; q++) ndo *= (uint32_t)J.ex[q] + 1;
     J.ndo = ndo;
+    // low group: the leading odd primes while their radix product stays <= sqrt(ndo)
+    uint32_t L = 1, js = J.j0;
+    while (js < J.np && L * ((uint32_t)J.ex[js] + 1) * L * ((uint32_t)J.ex[js] + 1) <= ndo) L *= (uint32_t)J.ex[js++] + 1;
+    J.js = js;
+    J.L = L;
+    J.H = ndo / L;
     const uint64_t nd = (uint64_t)ndo * (uint64_t)(J.E2 + 1);
     J.nd = (uint32_t)nd;
     // same-parity complementary pairs with f < g: the reference's ext_cand (s4.c:191)
@@ -360,7 +375,22 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
     return true;
 }
 
-// Square tests of queue entries [first, first+count), one per lane (s4.c:199-203).
+// divisors of prod pr[q]^ex[q], q in [q0, q1), in mixed-radix order (first prime fastest)
+__device__ __forceinline__ void gen_list(uint64_t *d, const uint32_t *pr, const uint8_t *ex, int q0, int q1) {
+    d[0] = 1;
+    uint32_t nn = 1;
+    for (int q = q0; q < q1; q++) {
+        const uint32_t cur = nn;
+        uint64_t pk = 1;
+        for (int e = 1; e <= ex[q]; e++) {
+            pk *= pr[q];
+            for (uint32_t i = 0; i < cur; i++) d[nn++] = d[i] * pk;
+        }
+    }
+}
+
+// Square tests of queue entries [first, first+count), one per lane (s4.c:199-203); a hit
+// gets its order key, the reference's mixed-radix index of the smaller divisor.
 __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, uint32_t first, uint32_t count,
                                               uint64_t bbase, int lane) {
     if ((uint32_t)lane < count) {
@@ -370,11 +400,17 @@ __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, 
         const EJob &J = w->job[jl];
         const u128 e = (u128)u * u - J.A;
         if (is_square_fast(e + J.C1) && is_square_fast(e + J.C2)) {
+            const uint32_t c = w->qidx[idx], l = c & 0xFFFu, h = (c >> 12) & 0xFFFu, d2 = c >> 24;
+            const uint64_t fo = w->dbuf[J.base + l] * w->dbuf[J.base + J.L + h];
+            const uint64_t go = w->dbuf[J.base + J.L - 1 - l] * w->dbuf[J.base + J.L + J.H - 1 - h];
+            const uint32_t to = l + J.L * h;
+            const uint32_t t = (J.flags & 1) ? d2 + (J.E2 + 1u) * to : to;
+            const uint32_t key = (fo << d2) < (go << (J.E2 - d2)) ? t : J.nd - 1 - t;
             const uint32_t slot = atomicAdd(&w->n_ext, 1u);
             if (slot < EXCAP) {
                 ExtEntry &x = w->ext[slot];
                 x.qid = (uint32_t)(bbase + jl);
-                x.key = w->qk[idx];
+                x.key = key;
                 x.lo = (uint64_t)e;
                 x.hi = (uint64_t)(e >> 64);
             } else {
@@ -411,21 +447,21 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
         // ---- phase A: one 4-set per lane
         LaneJob J;
         bool pending = jidx < njobs && job_setup(a, jidx, J);
-        const bool big = pending && J.ndo > (uint32_t)DCAP;
+        const bool big = pending && J.L + J.H > (uint32_t)DCAP;
         if (pending) {
             cnt.use(a, J.item);
             if (J.nd > cnt.mdiv) cnt.mdiv = J.nd;
             if (!big) cnt.cand += J.ncand;
         }
-        if (big) {                       // rare: more odd divisors than the warp buffer holds
+        if (big) {                       // extremely rare: its factored lists exceed the buffer
             uint32_t md = 0;
             extend_quad(a, J.r, J.v, J.S, J.bi, J.bj, J.bk, (uint32_t)jidx, cnt.cand, cnt.sqrt_, md, w->ext,
                         &w->n_ext, EXCAP);
             pending = false;
         }
         while (__any_sync(FULL, pending)) {
-            // place the divisor lists of as many pending lanes as fit, in lane order
-            const uint32_t want = pending ? J.ndo : 0;
+            // place the factored divisor lists of as many pending lanes as fit, in lane order
+            const uint32_t want = pending ? J.L + J.H : 0;
             uint32_t incl = want;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -435,35 +471,28 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             const uint32_t base = incl - want;
             const bool fits = pending && incl <= (uint32_t)DCAP;
             if (fits) {
-                // odd divisors in mixed-radix order over the odd primes: the reference's
-                // gen_divisors order (s4.c:149-156) restricted to the odd part
-                uint64_t *d = w->dbuf + base;
-                d[0] = 1;
-                uint32_t nn = 1;
-                for (int q = J.j0; q < J.np; q++) {
-                    const uint32_t cur = nn;
-                    uint64_t pk = 1;
-                    for (int e = 1; e <= J.ex[q]; e++) {
-                        pk *= J.pr[q];
-                        for (uint32_t i = 0; i < cur; i++) d[nn++] = d[i] * pk;
-                    }
-                }
+                gen_list(w->dbuf + base, J.pr, J.ex, J.j0, J.js);              // lo: L entries
+                gen_list(w->dbuf + base + J.L, J.pr, J.ex, J.js, J.np);        // hi: H entries
                 EJob &E = w->job[lane];
                 E.A = J.A; E.C1 = J.C1; E.C2 = J.C2;
                 const int64_t dd1 = (int64_t)J.C1 - (int64_t)J.A, dd2 = (int64_t)J.C2 - (int64_t)J.A;
-                E.m64a = rot64(QR64, smod(dd1, 64)); E.m64b = rot64(QR64, smod(dd2, 64));
-                E.m63a = rot63(QR63, smod(dd1, 63)); E.m63b = rot63(QR63, smod(dd2, 63));
-                uint32_t h1, h2;
-                rot65(smod(dd1, 65), E.m65a, h1);
-                rot65(smod(dd2, 65), E.m65b, h2);
+                uint32_t a63, a65, b63, b65, h1, h2;
+                res6365(dd1, a63, a65);
+                res6365(dd2, b63, b65);
+                E.m64 = rot64(QR64, (uint32_t)dd1 & 63u) & rot64(QR64, (uint32_t)dd2 & 63u);
+                E.m63 = rot63(QR63, a63) & rot63(QR63, b63);
+                uint64_t m65a, m65b;
+                rot65(a65, m65a, h1);
+                rot65(b65, m65b, h2);
+                E.m65 = m65a & m65b;
                 uint64_t vmax = J.v[0];
                 for (int i = 1; i < 4; i++) vmax = J.v[i] > vmax ? J.v[i] : vmax;
                 E.uA = isqrt64(J.A);
                 E.uS = isqrt64(J.A + vmax);
                 E.nd = J.nd; E.ncand = J.ncand; E.item = J.item;
-                E.base = (uint16_t)base; E.ndo = (uint16_t)J.ndo;
+                E.base = (uint16_t)base; E.L = (uint16_t)J.L; E.H = (uint16_t)J.H;
                 E.E2 = (uint8_t)J.E2;
-                E.flags = (uint8_t)((J.has2 ? 1 : 0) | (h1 << 1) | (h2 << 2));
+                E.flags = (uint8_t)((J.has2 ? 1 : 0) | ((h1 & h2) << 1));
             }
             // ---- phase B: the pooled candidates, 32 equal contiguous runs
             const uint32_t nc = fits ? J.ncand : 0;
@@ -490,42 +519,45 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 jl = lo;
             }
             // the current job of this lane's run, in registers
-            uint64_t A = 0, m64a = 0, m64b = 0, m63a = 0, m63b = 0, m65a = 0, m65b = 0, uA = 0, uS = 0;
-            uint32_t nd = 0, ncand = 0, jbase = 0, ndo = 0, E2 = 0, flg = 0, R = 1;
-            uint32_t cc = 0, t_odd = 0, d2 = 0;
+            uint64_t A = 0, m64 = 0, m63 = 0, m65 = 0, uA = 0, uS = 0, hv = 0, hc = 0;
+            uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1;
+            uint32_t cc = 0, l = 0, h = 0, d2 = 0, hcur = 0xFFFFFFFFu;
             auto load_job = [&](uint32_t j, uint32_t cidx) {
                 const EJob &E = w->job[j];
-                A = E.A; m64a = E.m64a; m64b = E.m64b; m63a = E.m63a; m63b = E.m63b; m65a = E.m65a; m65b = E.m65b;
-                uA = E.uA; uS = E.uS; nd = E.nd; ncand = E.ncand; jbase = E.base; ndo = E.ndo; E2 = E.E2;
+                A = E.A; m64 = E.m64; m63 = E.m63; m65 = E.m65;
+                uA = E.uA; uS = E.uS; ncand = E.ncand; jb = E.base; L = E.L; H = E.H; E2 = E.E2;
                 flg = E.flags;
                 cnt.use(a, E.item);
                 cc = cidx;
-                if (flg & 1) { R = E2 - 1; t_odd = cidx / R; d2 = 1 + cidx % R; }
-                else { R = 1; t_odd = cidx; d2 = 0; }
+                uint32_t to;
+                if (flg & 1) { R = E2 - 1; to = cidx / R; d2 = 1 + cidx % R; }
+                else { R = 1; to = cidx; d2 = 0; }
+                h = to / L;
+                l = to - h * L;
+                hcur = 0xFFFFFFFFu;
             };
             if (g0 < g1) load_job(jl, g0 - w->cstart[jl]);
             uint32_t qn = 0;
             for (uint32_t it = 0; it < iters; it++) {
                 bool pass = false;
                 uint64_t u = 0;
-                uint32_t key = 0, jcur = jl;               // the job of THIS candidate
+                uint32_t cidx = 0, jcur = jl;              // the job of THIS candidate
                 if (it < g1 - g0) {
-                    // candidate (t_odd, d2): f = 2^d2 * fo, g = 2^(E2-d2) * go with fo*go = D_odd
-                    const uint64_t fo = w->dbuf[jbase + t_odd], go = w->dbuf[jbase + ndo - 1 - t_odd];
-                    uint64_t f = fo << d2, g = go << (E2 - d2);
-                    const uint32_t t = (flg & 1) ? d2 + (E2 + 1) * t_odd : t_odd;
-                    key = t;                                // mixed-radix index of the smaller divisor
-                    if (f > g) { const uint64_t s = f; f = g; g = s; key = nd - 1 - t; }
-                    u = (f + g) >> 1;
-                    // e + C = u^2 + (C - A): residues mod 64, 63, 65 (s4.c:192-194)
-                    const uint32_t w64 = (uint32_t)u & 63u, s64 = (w64 * w64) & 63u;
-                    const uint32_t rr = (uint32_t)(u >> 24) + ((uint32_t)u & 0xFFFFFFu);   // 2^24 = 1 mod 63 and mod 65
-                    const uint32_t w63 = rr % 63u, s63 = (w63 * w63) % 63u;
-                    const uint32_t w65 = rr % 65u, s65 = (w65 * w65) % 65u;
-                    const uint32_t b65a = s65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65a >> s65) & 1u;
-                    const uint32_t b65b = s65 == 64u ? (flg >> 2) & 1u : (uint32_t)(m65b >> s65) & 1u;
-                    pass = ((m64a >> s64) & (m64b >> s64) & (m63a >> s63) & (m63b >> s63) & 1u) && (b65a & b65b) &&
-                           u > uA;
+                    if (h != hcur) {                        // the high factors change every L candidates
+                        hv = w->dbuf[jb + L + h];
+                        hc = w->dbuf[jb + L + H - 1 - h];
+                        hcur = h;
+                    }
+                    // f = 2^d2 * lo[l]*hi[h], g = 2^(E2-d2) * lo[L-1-l]*hi[H-1-h]: complementary divisors
+                    const uint64_t fo = w->dbuf[jb + l] * hv, go = w->dbuf[jb + L - 1 - l] * hc;
+                    u = ((fo << d2) + (go << (E2 - d2))) >> 1;
+                    // e + C = u^2 + (C - A): residues mod 64, 63, 65 for both C (s4.c:192-194)
+                    const uint32_t w64 = (uint32_t)u & 63u;
+                    const uint32_t rr = (uint32_t)(u >> 24) + ((uint32_t)u & 0xFFFFFFu);   // 2^24 = 1 mod 63, 65
+                    const uint32_t w63 = rr % 63u, w65 = rr % 65u;
+                    const uint32_t s64 = (w64 * w64) & 63u, s63 = (w63 * w63) % 63u, s65 = (w65 * w65) % 65u;
+                    const uint32_t b65 = s65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65 >> s65) & 1u;
+                    pass = (((m64 >> s64) & (m63 >> s63) & 1u) & b65) && u > uA;
                     if (pass && u <= uS) {                  // e <= max(v): rule out e in v (s4.c:197)
                         const uint64_t e = u * u - A;
                         uint32_t jr[6], jit;
@@ -534,10 +566,11 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                         quad_values(jr, v, Sq);
                         if (e == v[0] || e == v[1] || e == v[2] || e == v[3]) pass = false;
                     }
-                    if (pass) cnt.sqrt_++;
+                    if (pass) { cnt.sqrt_++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
-                    if (flg & 1) { if (++d2 > R) { d2 = 1; t_odd++; } }
-                    else t_odd++;
+                    if (flg & 1) {
+                        if (++d2 > R) { d2 = 1; if (++l == L) { l = 0; h++; } }
+                    } else if (++l == L) { l = 0; h++; }
                     if (++cc == ncand && it + 1 < g1 - g0) {
                         do { jl++; } while (jl < 31 && w->cstart[jl + 1] == w->cstart[jl]);
                         load_job(jl, 0);
@@ -547,7 +580,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 if (pass) {
                     const uint32_t pos = qn + __popc(m & ((1u << lane) - 1u));
                     w->qu[pos] = u;
-                    w->qk[pos] = key;
+                    w->qidx[pos] = cidx;
                     w->qj[pos] = (uint8_t)jcur;
                 }
                 qn += __popc(m);
