@@ -104,7 +104,7 @@ __device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t gid
 }
 
 template <int TL>
-__global__ void __launch_bounds__(BS, 1) gen_jobs(const SearchArgs a) {
+__global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
     using L = TileLayout<TL>;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ TileShared ts;
@@ -165,22 +165,25 @@ __global__ void __launch_bounds__(BS, 1) gen_jobs(const SearchArgs a) {
 
 constexpr int EBS = 256;                 // threads per CTA
 constexpr int EWARPS = EBS / 32;
-constexpr int DCAP = 384;                // divisor-list entries per warp (u64)
+constexpr int DCAP = 352;                // divisor-list entries per warp (u64)
 constexpr int QCAP = 64;                 // square-test queue per warp
-constexpr int EXCAP = 16;                // extensions per warp batch
+constexpr int EXCAP = 8;                 // extensions per warp batch
+constexpr int FSLOT = 16;                // prime slots per lane: m1's primes from 0, m2's from 8
 
 // The odd part D_odd of a difference is kept factored: its odd primes are split into a low
 // group (the first primes of the reference's order) and a high group, with divisor lists
 // lo[0..L) and hi[0..H) in mixed-radix order.  The odd divisor with mixed-radix index
 // t = l + L*h is lo[l]*hi[h], and its complement (index ndo-1-t) is lo[L-1-l]*hi[H-1-h]:
 // L+H entries instead of ndo = L*H.
-struct EJob {                            // one lane's 4-set, read by every lane in phase B
-    uint64_t A, C1, C2;                  // extend by D = A - B; the other two members C1, C2
+struct __align__(16) EJob {              // one lane's 4-set, read by every lane in phase B
     uint64_t m64, m63, m65;              // bit s: u^2 + (C - A) is a residue for both C (mod 64/63/65)
-    uint64_t uA, uS;                     // u <= uA: e <= 0;  u <= uS: e <= max(v)
-    uint32_t nd, ncand, item;
+    uint64_t A;                          // extend by D = A - B
+    uint32_t uA, uS;                     // u <= uA: e <= 0;  u <= uS: e <= max(v)
+    uint32_t ncand, item;
     uint16_t base, L, H;                 // lo list at dbuf[base..base+L), hi list right after it
     uint8_t E2, flags;                   // flags: 1 = D even, 2 = residue 64 passes mod 65
+    uint32_t nd, pad;
+    uint64_t C1, C2;                     // the other two members (square tests)
 };
 
 struct WarpArea {
@@ -191,8 +194,12 @@ struct WarpArea {
     uint64_t qu[QCAP];
     uint8_t qj[QCAP];
     ExtEntry ext[EXCAP];
+    uint32_t fp[FSLOT][32];              // each lane's primes of D, lane-minor (no bank conflicts)
+    uint8_t fe[FSLOT][32];               //   and their exponents
     uint32_t n_ext;
 };
+
+static_assert(EWARPS * sizeof(WarpArea) + 1024 <= 228 * 1024 / 3, "three engine CTAs per SM");
 
 // Rotated residue masks: bit s of the result is QR_m[(s + a) mod m], so the test of
 // e + C = u^2 + (C - A) becomes one shift of the mask by u^2 mod m.
@@ -329,16 +336,61 @@ struct LaneJob {
     uint32_t r[6], item;
     uint64_t v[4], S, A, C1, C2;
     int bi, bj, bk;
-    uint32_t pr[MAXP];
-    uint8_t ex[MAXP];
-    int np;
+    int np;                              // distinct primes, in w->fp/fe[0..np)[lane]
     bool has2;
     int E2, j0, js;                      // odd primes are pr[j0..np); the high group starts at js
     uint32_t ndo, nd, ncand, L, H;
 };
 
 // Returns false if the 4-set's difference has more divisors than cap_divs (fatal).
-__device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJob &J) {
+// Factor D = m1*m2 (m1 = ra-rb, m2 = ra+rb, both < 2^23, so at most 7 distinct primes each):
+// the two smallest-prime-factor walks run interleaved so that their dependent table loads
+// overlap; m1's primes are stored from slot 0, m2's from slot 8, then m2's are merged into
+// m1's list -- primes in first-seen order, as s4.c:141-147.  A new prime is written to a slot
+// below every unread slot of m2, so the merge is in place.
+__device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, uint32_t m2, uint32_t (*fp)[32],
+                                           uint8_t (*fe)[32], int lane) {
+    int na = 0, nb = 0;
+    uint32_t pa = 0, pb = 0, ea = 0, eb = 0;
+    uint64_t sa = m1 > 1 ? __ldg(&spfq[m1]) : 0, sb = m2 > 1 ? __ldg(&spfq[m2]) : 0;
+    while (m1 > 1 || m2 > 1) {
+        if (m1 > 1) {
+            const uint32_t p = (uint32_t)sa;
+            if (p != pa) {
+                if (ea) { fp[na][lane] = pa; fe[na][lane] = (uint8_t)ea; na++; }
+                pa = p; ea = 0;
+            }
+            ea++;
+            m1 = (uint32_t)(sa >> 32);
+            if (m1 > 1) sa = __ldg(&spfq[m1]);
+        }
+        if (m2 > 1) {
+            const uint32_t p = (uint32_t)sb;
+            if (p != pb) {
+                if (eb) { fp[8 + nb][lane] = pb; fe[8 + nb][lane] = (uint8_t)eb; nb++; }
+                pb = p; eb = 0;
+            }
+            eb++;
+            m2 = (uint32_t)(sb >> 32);
+            if (m2 > 1) sb = __ldg(&spfq[m2]);
+        }
+    }
+    if (ea) { fp[na][lane] = pa; fe[na][lane] = (uint8_t)ea; na++; }
+    if (eb) { fp[8 + nb][lane] = pb; fe[8 + nb][lane] = (uint8_t)eb; nb++; }
+    int np = na;
+    for (int j = 0; j < nb; j++) {
+        const uint32_t p = fp[8 + j][lane];
+        const uint8_t e = fe[8 + j][lane];
+        int i = 0;
+        while (i < na && fp[i][lane] != p) i++;
+        if (i < na) fe[i][lane] = (uint8_t)(fe[i][lane] + e);
+        else { fp[np][lane] = p; fe[np][lane] = e; np++; }
+    }
+    return np;
+}
+
+__device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJob &J, uint32_t (*fp)[32],
+                                          uint8_t (*fe)[32], int lane) {
     get_job(a.jobs, a.jobs_cap, j, J.r, J.item);
     quad_values(J.r, J.v, J.S);
     uint32_t best;
@@ -351,19 +403,18 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
         if (t != J.bi && t != J.bj) { if (o1 < 0) o1 = t; else o2 = t; }
     J.C1 = pick4(J.v, o1);
     J.C2 = pick4(J.v, o2);
-    J.np = 0;
-    factor_merge(a.spfq, ra - rb, J.pr, J.ex, J.np);
-    factor_merge(a.spfq, ra + rb, J.pr, J.ex, J.np);
+    J.np = factor_pair(a.spfq, ra - rb, ra + rb, fp, fe, lane);
     // D even => both factors even => 2 is the first prime and 4 | D
-    J.has2 = J.np > 0 && J.pr[0] == 2;
-    J.E2 = J.has2 ? J.ex[0] : 0;
+    J.has2 = J.np > 0 && fp[0][lane] == 2;
+    J.E2 = J.has2 ? fe[0][lane] : 0;
     J.j0 = J.has2 ? 1 : 0;
     uint32_t ndo = 1;
-    for (int q = J.j0; q < J.np; q++) ndo *= (uint32_t)J.ex[q] + 1;
+    for (int q = J.j0; q < J.np; q++) ndo *= (uint32_t)fe[q][lane] + 1;
     J.ndo = ndo;
     // low group: the leading odd primes while their radix product stays <= sqrt(ndo)
     uint32_t L = 1, js = J.j0;
-    while (js < J.np && L * ((uint32_t)J.ex[js] + 1) * L * ((uint32_t)J.ex[js] + 1) <= ndo) L *= (uint32_t)J.ex[js++] + 1;
+    while (js < J.np && L * ((uint32_t)fe[js][lane] + 1) * L * ((uint32_t)fe[js][lane] + 1) <= ndo)
+        L *= (uint32_t)fe[js++][lane] + 1;
     J.js = js;
     J.L = L;
     J.H = ndo / L;
@@ -376,17 +427,25 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
 }
 
 // divisors of prod pr[q]^ex[q], q in [q0, q1), in mixed-radix order (first prime fastest)
-__device__ __forceinline__ void gen_list(uint64_t *d, const uint32_t *pr, const uint8_t *ex, int q0, int q1) {
+__device__ __forceinline__ void gen_list(uint64_t *d, const uint32_t (*fp)[32], const uint8_t (*fe)[32], int lane,
+                                         int q0, int q1) {
     d[0] = 1;
     uint32_t nn = 1;
     for (int q = q0; q < q1; q++) {
-        const uint32_t cur = nn;
+        const uint32_t cur = nn, pq = fp[q][lane], eq = fe[q][lane];
         uint64_t pk = 1;
-        for (int e = 1; e <= ex[q]; e++) {
-            pk *= pr[q];
+        for (uint32_t e = 1; e <= eq; e++) {
+            pk *= pq;
             for (uint32_t i = 0; i < cur; i++) d[nn++] = d[i] * pk;
         }
     }
+}
+
+// A 4-set whose factored divisor lists exceed the warp buffer: the per-lane divisor walk.
+static __device__ __noinline__ void extend_big(const SearchArgs &a, const LaneJob &J, uint32_t qid, ull &cand,
+                                               ull &sq, ExtEntry *el, uint32_t *el_n) {
+    uint32_t md = 0;
+    extend_quad(a, J.r, J.v, J.S, J.bi, J.bj, J.bk, qid, cand, sq, md, el, el_n, EXCAP);
 }
 
 // Square tests of queue entries [first, first+count), one per lane (s4.c:199-203); a hit
@@ -446,7 +505,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
 
         // ---- phase A: one 4-set per lane
         LaneJob J;
-        bool pending = jidx < njobs && job_setup(a, jidx, J);
+        bool pending = jidx < njobs && job_setup(a, jidx, J, w->fp, w->fe, lane);
         const bool big = pending && J.L + J.H > (uint32_t)DCAP;
         if (pending) {
             cnt.use(a, J.item);
@@ -454,9 +513,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             if (!big) cnt.cand += J.ncand;
         }
         if (big) {                       // extremely rare: its factored lists exceed the buffer
-            uint32_t md = 0;
-            extend_quad(a, J.r, J.v, J.S, J.bi, J.bj, J.bk, (uint32_t)jidx, cnt.cand, cnt.sqrt_, md, w->ext,
-                        &w->n_ext, EXCAP);
+            extend_big(a, J, (uint32_t)jidx, cnt.cand, cnt.sqrt_, w->ext, &w->n_ext);
             pending = false;
         }
         while (__any_sync(FULL, pending)) {
@@ -471,8 +528,8 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             const uint32_t base = incl - want;
             const bool fits = pending && incl <= (uint32_t)DCAP;
             if (fits) {
-                gen_list(w->dbuf + base, J.pr, J.ex, J.j0, J.js);              // lo: L entries
-                gen_list(w->dbuf + base + J.L, J.pr, J.ex, J.js, J.np);        // hi: H entries
+                gen_list(w->dbuf + base, w->fp, w->fe, lane, J.j0, J.js);              // lo: L entries
+                gen_list(w->dbuf + base + J.L, w->fp, w->fe, lane, J.js, J.np);        // hi: H entries
                 EJob &E = w->job[lane];
                 E.A = J.A; E.C1 = J.C1; E.C2 = J.C2;
                 const int64_t dd1 = (int64_t)J.C1 - (int64_t)J.A, dd2 = (int64_t)J.C2 - (int64_t)J.A;
@@ -487,8 +544,8 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 E.m65 = m65a & m65b;
                 uint64_t vmax = J.v[0];
                 for (int i = 1; i < 4; i++) vmax = J.v[i] > vmax ? J.v[i] : vmax;
-                E.uA = isqrt64(J.A);
-                E.uS = isqrt64(J.A + vmax);
+                E.uA = (uint32_t)isqrt64(J.A);                  // < 2^22 (A < 2^44)
+                E.uS = (uint32_t)isqrt64(J.A + vmax);           // < 2^23
                 E.nd = J.nd; E.ncand = J.ncand; E.item = J.item;
                 E.base = (uint16_t)base; E.L = (uint16_t)J.L; E.H = (uint16_t)J.H;
                 E.E2 = (uint8_t)J.E2;
@@ -519,35 +576,40 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 jl = lo;
             }
             // the current job of this lane's run, in registers
-            uint64_t A = 0, m64 = 0, m63 = 0, m65 = 0, uA = 0, uS = 0, hv = 0, hc = 0;
+            uint64_t A = 0, m64 = 0, m63 = 0, m65 = 0, hv = 0, hc = 0;
+            uint32_t uA = 0, uS = 0;
             uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1;
-            uint32_t cc = 0, l = 0, h = 0, d2 = 0, hcur = 0xFFFFFFFFu;
-            auto load_job = [&](uint32_t j, uint32_t cidx) {
-                const EJob &E = w->job[j];
-                A = E.A; m64 = E.m64; m63 = E.m63; m65 = E.m65;
-                uA = E.uA; uS = E.uS; ncand = E.ncand; jb = E.base; L = E.L; H = E.H; E2 = E.E2;
-                flg = E.flags;
-                cnt.use(a, E.item);
-                cc = cidx;
-                uint32_t to;
-                if (flg & 1) { R = E2 - 1; to = cidx / R; d2 = 1 + cidx % R; }
-                else { R = 1; to = cidx; d2 = 0; }
+            uint32_t cc = 0, l = 0, h = 0, d2 = 0;
+            // job fields in four vector loads; entering a job at its first candidate needs no division
+            auto load_job = [&](uint32_t j) {
+                const ulonglong2 *E2p = (const ulonglong2 *)&w->job[j];
+                const ulonglong2 x0 = E2p[0], x1 = E2p[1];
+                const uint4 y = *(const uint4 *)&w->job[j].uA;
+                const uint2 z = *(const uint2 *)&w->job[j].base;
+                m64 = x0.x; m63 = x0.y; m65 = x1.x; A = x1.y;
+                uA = y.x; uS = y.y; ncand = y.z;
+                jb = z.x & 0xFFFFu; L = z.x >> 16; H = z.y & 0xFFFFu; E2 = (z.y >> 16) & 0xFFu; flg = z.y >> 24;
+                R = (flg & 1) ? E2 - 1 : 1;
+                cnt.use(a, y.w);
+                cc = 0; l = 0; h = 0; d2 = (flg & 1) ? 1u : 0u;
+            };
+            if (g0 < g1) {
+                load_job(jl);
+                const uint32_t cidx = g0 - w->cstart[jl];
+                const uint32_t to = (flg & 1) ? cidx / R : cidx;
+                d2 = (flg & 1) ? 1 + cidx % R : 0;
                 h = to / L;
                 l = to - h * L;
-                hcur = 0xFFFFFFFFu;
-            };
-            if (g0 < g1) load_job(jl, g0 - w->cstart[jl]);
+                cc = cidx;
+            }
             uint32_t qn = 0;
             for (uint32_t it = 0; it < iters; it++) {
                 bool pass = false;
                 uint64_t u = 0;
                 uint32_t cidx = 0, jcur = jl;              // the job of THIS candidate
                 if (it < g1 - g0) {
-                    if (h != hcur) {                        // the high factors change every L candidates
-                        hv = w->dbuf[jb + L + h];
-                        hc = w->dbuf[jb + L + H - 1 - h];
-                        hcur = h;
-                    }
+                    hv = w->dbuf[jb + L + h];
+                    hc = w->dbuf[jb + L + H - 1 - h];
                     // f = 2^d2 * lo[l]*hi[h], g = 2^(E2-d2) * lo[L-1-l]*hi[H-1-h]: complementary divisors
                     const uint64_t fo = w->dbuf[jb + l] * hv, go = w->dbuf[jb + L - 1 - l] * hc;
                     u = ((fo << d2) + (go << (E2 - d2))) >> 1;
@@ -573,7 +635,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     } else if (++l == L) { l = 0; h++; }
                     if (++cc == ncand && it + 1 < g1 - g0) {
                         do { jl++; } while (jl < 31 && w->cstart[jl + 1] == w->cstart[jl]);
-                        load_job(jl, 0);
+                        load_job(jl);
                     }
                 }
                 const unsigned m = __ballot_sync(FULL, pass);
@@ -607,7 +669,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
 
 // ================================================================== launchers
 
-int gen_grid(int num_sms) { return num_sms; }
+int gen_grid(int num_sms) { return 2 * num_sms; }     // two 100 KB tile CTAs per SM
 int ext_grid(int num_sms) { return num_sms * 3; }
 
 template <int TL>
