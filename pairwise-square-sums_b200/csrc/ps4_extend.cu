@@ -182,7 +182,7 @@ struct __align__(16) EJob {              // one lane's 4-set, read by every lane
     uint32_t ncand, item;
     uint16_t base, L, H;                 // lo list at dbuf[base..base+L), hi list right after it
     uint8_t E2, flags;                   // flags: 1 = D even, 2 = residue 64 passes mod 65
-    uint32_t nd, pad;
+    uint64_t B;                          // the smaller member of the difference (e in v check)
     uint64_t C1, C2;                     // the other two members (square tests)
 };
 
@@ -214,6 +214,15 @@ __device__ __forceinline__ void rot65(uint32_t a, uint64_t &lo, uint32_t &bit64)
     const u128 Y = a ? ((X >> a) | (X << (65 - a))) & M : X;
     lo = (uint64_t)Y;
     bit64 = (uint32_t)(Y >> 64) & 1u;
+}
+
+// floor(sqrt(x)) for x < 2^46: a float estimate is within one unit of the root (the root is
+// < 2^23, and float carries 24 bits), then exact integer correction.
+__device__ __forceinline__ uint32_t isqrt_lt2p46(uint64_t x) {
+    uint32_t r = (uint32_t)sqrtf((float)x);
+    while ((uint64_t)r * r > x) r--;
+    while ((uint64_t)(r + 1) * (r + 1) <= x) r++;
+    return r;
 }
 
 // (d mod 63, d mod 65) for |d| < 2^48, by folding 24-bit halves (2^24 = 1 mod 63 and mod 65)
@@ -464,7 +473,8 @@ __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, 
             const uint64_t go = w->dbuf[J.base + J.L - 1 - l] * w->dbuf[J.base + J.L + J.H - 1 - h];
             const uint32_t to = l + J.L * h;
             const uint32_t t = (J.flags & 1) ? d2 + (J.E2 + 1u) * to : to;
-            const uint32_t key = (fo << d2) < (go << (J.E2 - d2)) ? t : J.nd - 1 - t;
+            const uint32_t nd = (uint32_t)J.L * J.H * ((J.flags & 1) ? J.E2 + 1u : 1u);
+            const uint32_t key = (fo << d2) < (go << (J.E2 - d2)) ? t : nd - 1 - t;
             const uint32_t slot = atomicAdd(&w->n_ext, 1u);
             if (slot < EXCAP) {
                 ExtEntry &x = w->ext[slot];
@@ -544,9 +554,9 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 E.m65 = m65a & m65b;
                 uint64_t vmax = J.v[0];
                 for (int i = 1; i < 4; i++) vmax = J.v[i] > vmax ? J.v[i] : vmax;
-                E.uA = (uint32_t)isqrt64(J.A);                  // < 2^22 (A < 2^44)
-                E.uS = (uint32_t)isqrt64(J.A + vmax);           // < 2^23
-                E.nd = J.nd; E.ncand = J.ncand; E.item = J.item;
+                E.uA = isqrt_lt2p46(J.A);                        // < 2^22 (A < 2^44)
+                E.uS = isqrt_lt2p46(J.A + vmax);                 // < 2^23
+                E.B = pick4(J.v, J.bj); E.ncand = J.ncand; E.item = J.item;
                 E.base = (uint16_t)base; E.L = (uint16_t)J.L; E.H = (uint16_t)J.H;
                 E.E2 = (uint8_t)J.E2;
                 E.flags = (uint8_t)((J.has2 ? 1 : 0) | ((h1 & h2) << 1));
@@ -621,12 +631,9 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     const uint32_t b65 = s65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65 >> s65) & 1u;
                     pass = (((m64 >> s64) & (m63 >> s63) & 1u) & b65) && u > uA;
                     if (pass && u <= uS) {                  // e <= max(v): rule out e in v (s4.c:197)
-                        const uint64_t e = u * u - A;
-                        uint32_t jr[6], jit;
-                        get_job(a.jobs, a.jobs_cap, bbase + jcur, jr, jit);
-                        uint64_t v[4], Sq;
-                        quad_values(jr, v, Sq);
-                        if (e == v[0] || e == v[1] || e == v[2] || e == v[3]) pass = false;
+                        const uint64_t e = u * u - A;       // u < 2^23
+                        const EJob &Ej = w->job[jcur];
+                        if (e == A || e == Ej.B || e == Ej.C1 || e == Ej.C2) pass = false;
                     }
                     if (pass) { cnt.sqrt_++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
