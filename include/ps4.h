@@ -169,6 +169,38 @@ void ps4_last_transfer_bytes(const ps4_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
  * caller.  Synchronous on the context's stream. */
 int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res);
 
+/* ---- triple extension ----
+ *
+ * For each triple {a, b, c} of distinct positive integers whose three pairwise sums are
+ * squares, every d with 0 < d <= dmax, d not in the triple, and d+a, d+b, d+c all squares.
+ * The reference runs this step only inside its search, on 4-sets: extend4 (exhaustive/s4.c:
+ * 160-207) with the same divisor-pair construction -- e + A = u^2, e + B = w^2 gives
+ * (u - w)(u + w) = A - B, enumerated through the factorisation of A - B = r_AC^2 - r_BC^2
+ * -- and its pair choice by estimated divisor count (s4.c:163-171). */
+typedef struct {
+    uint64_t d;           /* the extension                                                        */
+    uint32_t item;        /* index of the triple in the call's input                              */
+    uint32_t reserved;    /* 0                                                                    */
+} ps4_tri_ext;
+
+typedef struct {
+    uint64_t triples;     /* triples searched (valid ones)                                        */
+    uint64_t invalid;     /* inputs that are not a square-sum triple of distinct positive integers */
+    uint64_t ext_cand;    /* same-parity complementary divisor pairs f < g enumerated (ext_cand)  */
+    uint64_t ext_sqrt;    /* exact square tests of d + C after the residue filters                */
+    uint64_t exts;        /* extensions found                                                     */
+} ps4_tri_stats;
+
+/* abc holds 3*n members (triple i = abc[3i..3i+2], any order); state (n bytes, may be NULL)
+ * receives 0 for a searched triple and 1 for an input that is not a square-sum triple of
+ * distinct positive integers (no records; the oracle returns -1 for those).  Members must
+ * stay below 2^44 and their pairwise-sum roots inside the context's factor tables (largest
+ * member <= s_hi_max / 2 is always enough), dmax <= 2^62; otherwise PS4_ERR_ARG.  Records
+ * are sorted by (item, d); stats (+=, may be NULL).  More records than out_cap give
+ * PS4_ERR_OUTPUT_FULL with *n_out the needed count.  Synchronous on the context's stream. */
+int ps4_extend_triples(ps4_ctx *ctx, const uint64_t *abc, uint32_t n, uint64_t dmax, uint8_t *state,
+                       ps4_tri_ext *out, uint64_t out_cap, uint64_t *n_out, ps4_tri_stats *stats);
+
 /* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
 double ps4_last_kernel_ms(const ps4_ctx *ctx);
 /* Number of kernel launches made by the last search call. */

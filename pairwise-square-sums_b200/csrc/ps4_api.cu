@@ -55,6 +55,11 @@ struct ps4_ctx {
     uint32_t batch_div = 1;              // narrows the batches after a queue overflow
     bool fused_fallback = false;         // this call re-runs on the fused kernel (engine list overflow)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    // triple extension (grown on demand)
+    uint64_t *d_tri_in = nullptr; uint64_t tri_in_cap = 0;
+    uint8_t *d_tri_state = nullptr; uint64_t tri_state_cap = 0;
+    ps4_tri_ext *d_tri_out = nullptr; uint64_t tri_out_cap = 0;
+    unsigned long long *d_tri_cnt = nullptr; uint64_t tri_cnt_cap = 0;   // n_out, n_cand, n_sqrt
     std::string err;
 };
 
@@ -114,6 +119,7 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     cudaFree(c->d_spfq); cudaFree(c->d_ndiv); cudaFree(c->d_items); cudaFree(c->d_counters);
     cudaFree(c->d_hits); cudaFree(c->d_exts); cudaFree(c->d_sixes); cudaFree(c->d_quads);
     cudaFree(c->d_scratch); cudaFree(c->d_status); cudaFree(c->d_jobs);
+    cudaFree(c->d_tri_in); cudaFree(c->d_tri_state); cudaFree(c->d_tri_out); cudaFree(c->d_tri_cnt);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -523,6 +529,87 @@ extern "C" int ps4_search_finish(ps4_ctx *c, ps4_stats *stats, ps4_results *res)
 extern "C" void ps4_last_transfer_bytes(const ps4_ctx *c, uint64_t *h2d, uint64_t *d2h) {
     if (h2d) *h2d = c ? c->h2d_bytes : 0;
     if (d2h) *d2h = c ? c->d2h_bytes : 0;
+}
+
+// ---- triple extension ----
+
+extern "C" int ps4_extend_triples(ps4_ctx *c, const uint64_t *abc, uint32_t n, uint64_t dmax, uint8_t *state,
+                                  ps4_tri_ext *out, uint64_t out_cap, uint64_t *n_out, ps4_tri_stats *stats) {
+    if (!c) return PS4_ERR_ARG;
+    if (c->pend.active) return set_err(c, PS4_ERR_ARG, "a search is enqueued on this context");
+    if (n_out) *n_out = 0;
+    c->last_launches = 0;
+    c->last_ms = 0.0;
+    c->h2d_bytes = c->d2h_bytes = 0;
+    if (n == 0) return PS4_OK;
+    if (!abc) return set_err(c, PS4_ERR_ARG, "ps4_extend_triples: no input");
+    if (dmax > (1ull << 62)) return set_err(c, PS4_ERR_ARG, "dmax %llu exceeds 2^62", (unsigned long long)dmax);
+    if (grow(c, c->d_tri_in, c->tri_in_cap, 3 * (uint64_t)n)) return PS4_ERR_CUDA;
+    if (grow(c, c->d_tri_state, c->tri_state_cap, n)) return PS4_ERR_CUDA;
+    if (grow(c, c->d_tri_cnt, c->tri_cnt_cap, 3)) return PS4_ERR_CUDA;
+    if (grow(c, c->d_tri_out, c->tri_out_cap, std::max<uint64_t>(c->tri_out_cap, std::max<uint64_t>(out_cap, 1u << 16))))
+        return PS4_ERR_CUDA;
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_tri_in, abc, 3 * (size_t)n * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+    c->h2d_bytes += 3 * (uint64_t)n * sizeof(uint64_t);
+    unsigned long long cnt[3];
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CUDA_TRY(c, cudaMemsetAsync(c->d_tri_cnt, 0, 3 * sizeof(unsigned long long), c->stream));
+        TriArgs t;
+        t.abc = c->d_tri_in; t.n = n; t.dmax = dmax;
+        t.spfq = c->d_spfq; t.ndiv = c->d_ndiv; t.tab_n = c->tab_n;
+        t.state = c->d_tri_state;
+        t.out = c->d_tri_out; t.out_cap = c->tri_out_cap;
+        t.n_out = c->d_tri_cnt; t.n_cand = c->d_tri_cnt + 1; t.n_sqrt = c->d_tri_cnt + 2;
+        t.item_base = 0;
+        CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
+        CUDA_TRY(c, (cudaError_t)launch_triples(t, c->stream));
+        CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
+        c->last_launches++;
+        CUDA_TRY(c, cudaMemcpyAsync(cnt, c->d_tri_cnt, sizeof cnt, cudaMemcpyDeviceToHost, c->stream));
+        CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+        c->d2h_bytes += sizeof cnt;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        c->last_ms = ms;
+        if (cnt[0] <= c->tri_out_cap) break;
+        // more records than the device buffer holds: grow it and run again (results do not
+        // depend on the buffer)
+        if (grow(c, c->d_tri_out, c->tri_out_cap, cnt[0] * 3 / 2 + 1024)) return PS4_ERR_CUDA;
+    }
+    std::vector<uint8_t> st(n);
+    CUDA_TRY(c, cudaMemcpyAsync(st.data(), c->d_tri_state, n, cudaMemcpyDeviceToHost, c->stream));
+    std::vector<ps4_tri_ext> recs(cnt[0]);
+    if (cnt[0])
+        CUDA_TRY(c, cudaMemcpyAsync(recs.data(), c->d_tri_out, cnt[0] * sizeof(ps4_tri_ext), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+    c->d2h_bytes += n + cnt[0] * sizeof(ps4_tri_ext);
+    uint64_t n_invalid = 0;
+    for (uint32_t i = 0; i < n; i++) {
+        if (st[i] == TRI_RANGE)
+            return set_err(c, PS4_ERR_ARG,
+                           "triple %u (%llu, %llu, %llu) is beyond the context's factor tables (s_hi_max %llu)", i,
+                           (unsigned long long)abc[3 * i], (unsigned long long)abc[3 * i + 1],
+                           (unsigned long long)abc[3 * i + 2], (unsigned long long)c->cfg.s_hi_max);
+        n_invalid += st[i] == TRI_INVALID;
+    }
+    if (state) memcpy(state, st.data(), n);
+    std::sort(recs.begin(), recs.end(), [](const ps4_tri_ext &x, const ps4_tri_ext &y) {
+        return x.item != y.item ? x.item < y.item : x.d < y.d;
+    });
+    if (n_out) *n_out = cnt[0];
+    if (cnt[0] > out_cap)
+        return set_err(c, PS4_ERR_OUTPUT_FULL, "triple output holds %llu records, %llu needed",
+                       (unsigned long long)out_cap, cnt[0]);
+    if (cnt[0]) memcpy(out, recs.data(), cnt[0] * sizeof(ps4_tri_ext));
+    if (stats) {
+        stats->triples += n - n_invalid;
+        stats->invalid += n_invalid;
+        stats->ext_cand += cnt[1];
+        stats->ext_sqrt += cnt[2];
+        stats->exts += cnt[0];
+    }
+    return PS4_OK;
 }
 
 // ---- read-only view of a context for the allocation-free entry point (ps4_kernels.cu) ----

@@ -74,6 +74,24 @@ struct SearchArgs {
     uint64_t jobs_cap;
 };
 
+// Arguments of one triple-extension launch (ps4_triples.cu).
+struct TriArgs {
+    const uint64_t *abc;       // 3 members per triple, any order
+    uint64_t n;                // triples
+    uint64_t dmax;             // extensions d <= dmax
+    const uint64_t *spfq;
+    const uint16_t *ndiv;
+    uint64_t tab_n;
+    uint8_t *state;            // per triple: TRI_OK / TRI_INVALID / TRI_RANGE
+    ps4_tri_ext *out;
+    uint64_t out_cap;
+    unsigned long long *n_out;     // records found (may exceed out_cap: nothing written past it)
+    unsigned long long *n_cand;    // same-parity complementary divisor pairs of the chosen differences
+    unsigned long long *n_sqrt;    // exact square tests of d + C
+    uint32_t item_base;            // added to the triple index in the records
+};
+enum { TRI_OK = 0, TRI_INVALID = 1, TRI_RANGE = 2 };
+
 // Read-only view of a context (ps4_api.cu), for the allocation-free entry point.
 struct CtxView {
     const uint64_t *spfq;
@@ -94,6 +112,7 @@ int launch_ext(const SearchArgs &a, int grid, void *stream);
 int gen_grid(int num_sms);
 int ext_grid(int num_sms);
 int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);
+int launch_triples(const TriArgs &t, void *stream);
 size_t search_smem_bytes(int kernel, unsigned log2_tile);
 int search_block_threads();
 uint32_t stage_cap_for(unsigned log2_tile, uint32_t cap_reps);

@@ -80,6 +80,18 @@ class Quad(C.Structure):
                 ("r_bd", C.c_uint32), ("r_cd", C.c_uint32)]
 
 
+class TriExt(C.Structure):
+    _fields_ = [("d", C.c_uint64), ("item", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class TriStats(C.Structure):
+    _fields_ = [("triples", C.c_uint64), ("invalid", C.c_uint64), ("ext_cand", C.c_uint64),
+                ("ext_sqrt", C.c_uint64), ("exts", C.c_uint64)]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_}
+
+
 class Results(C.Structure):
     _fields_ = [("hits", C.POINTER(Hit)), ("hits_cap", C.c_uint64), ("n_hits", C.c_uint64),
                 ("exts", C.POINTER(Ext)), ("exts_cap", C.c_uint64), ("n_exts", C.c_uint64),
@@ -114,6 +126,8 @@ def load() -> C.CDLL:
         "ps4_search_enqueue": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
         "ps4_search_finish": (C.c_int, [C.c_void_p, P(Stats), P(Results)]),
         "ps4_last_transfer_bytes": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
+        "ps4_extend_triples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,
+                                         C.c_uint64, P(C.c_uint64), P(TriStats)]),
         "ps4_format_hit": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),
         "ps4_format_six": (C.c_long, [P(Hit), P(Ext), P(Six), C.c_char_p, C.c_size_t]),
         "ps4_format_drill": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),

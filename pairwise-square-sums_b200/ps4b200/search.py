@@ -167,6 +167,37 @@ class Search:
             self._collect(out)
         return [s.as_dict() for s in st], out
 
+    def extend_triples(self, abc, dmax: int):
+        """Every d <= dmax extending each square-sum triple (rows of ``abc``) to a 4-set.
+
+        Returns (exts, state, stats): exts[i] the sorted extensions of triple i, state[i] 0 for
+        a searched triple and 1 for a row that is not a square-sum triple of distinct positive
+        integers, stats the call's counters."""
+        import numpy as np
+        a = np.ascontiguousarray(np.asarray(abc, dtype=np.uint64).reshape(-1, 3))
+        n = a.shape[0]
+        state = np.zeros(max(n, 1), dtype=np.uint8)
+        cap = max(self._tri_cap, 1024) if hasattr(self, "_tri_cap") else 1 << 16
+        st = _abi.TriStats()
+        while True:
+            out = (_abi.TriExt * cap)()
+            n_out = C.c_uint64()
+            rc = self.lib.ps4_extend_triples(self.ctx, a.ctypes.data, n, int(dmax), state.ctypes.data, out, cap,
+                                             C.byref(n_out), C.byref(st))
+            if rc == _abi.PS4_ERR_OUTPUT_FULL:
+                cap = int(n_out.value) * 3 // 2 + 1024
+                continue
+            if rc != _abi.PS4_OK:
+                raise Ps4Error(rc, self.lib.ps4_last_error(self.ctx).decode())
+            break
+        self._tri_cap = cap
+        recs = np.frombuffer(out, dtype=np.dtype([("d", "<u8"), ("item", "<u4"), ("reserved", "<u4")]),
+                             count=int(n_out.value))
+        exts = [[] for _ in range(n)]
+        for d, item in zip(recs["d"].tolist(), recs["item"].tolist()):
+            exts[item].append(d)
+        return exts, state[:n], st.as_dict()
+
     def _collect(self, out: RangeResult):
         r = self._res
         buf = C.create_string_buffer(_LINE_CAP)
