@@ -201,6 +201,69 @@ typedef struct {
 int ps4_extend_triples(ps4_ctx *ctx, const uint64_t *abc, uint32_t n, uint64_t dmax, uint8_t *state,
                        ps4_tri_ext *out, uint64_t out_cap, uint64_t *n_out, ps4_tri_stats *stats);
 
+/* ---- serving: continuous batching of subrange and triple queries ----
+ *
+ * The reference serves its search as one s4 process per block from a Python controller
+ * (run_exhaustive.py:200-238, one subprocess per block, results parsed from stdout) and has
+ * no triple query.  A server replaces that loop in-process: queries are submitted as they
+ * arrive, admitted while a device slot and room in a fixed device-memory budget are free, and
+ * run in steps -- each step one launch of the search kernels over chunks of every admitted
+ * subrange (shortest remaining first, the oldest always included) plus one triple-extension
+ * launch over every admitted triple query -- so queries that arrive while others run join
+ * the next step and share its kernels.  Counters and result records of each query accumulate
+ * on the device in its slot; a finished query's results are copied to the host once.  Each
+ * query's results are the ones ps4_search_range / ps4_extend_triples give for it alone.
+ * One host thread per server; the context's tables are shared read-only. */
+typedef struct ps4_server ps4_server;
+
+typedef struct {
+    uint64_t hbm_budget;        /* device bytes for the server: step buffers + per-query arena (0 = 8 GiB) */
+    uint32_t max_slots;         /* queries resident on the device at once (0 = 1024)                      */
+    uint32_t max_step_items;    /* subrange chunks per step (0 = 4096)                                    */
+    uint64_t step_S;            /* S values per step over all chunks (0 = 2^27)                           */
+    uint32_t max_step_triples;  /* triple queries per step (0 = 65536)                                    */
+    uint32_t hits_floor;        /* result-buffer quota of a subrange query: hits_floor + hits_per_1e6_S    */
+    uint32_t hits_per_1e6_S;    /*   hits per million S, extensions twice that (0, 0 = 256, 40); a query   */
+    uint32_t reserved;          /*   that outgrows its quota is re-admitted with larger buffers and re-run */
+} ps4_serve_config;
+
+enum { PS4_Q_RANGE = 0, PS4_Q_TRIPLE = 1 };
+
+typedef struct {              /* one finished query, reported by ps4_serve_progress                     */
+    uint64_t tag;             /* the caller's tag given at submit                                       */
+    int32_t status;           /* PS4_OK or the error the same query alone would give                    */
+    uint32_t kind;            /* PS4_Q_*                                                                */
+    uint64_t n_records;       /* hits (subrange) or extensions (triple)                                 */
+    double t_submit, t_admit, t_done;   /* host monotonic clock (CLOCK_MONOTONIC), seconds              */
+    uint32_t steps;           /* steps that carried work of this query                                  */
+    uint32_t reruns;          /* re-runs after its device result buffers overflowed                     */
+    char message[160];        /* error text when status != PS4_OK                                       */
+} ps4_serve_done;
+
+typedef struct {
+    uint64_t submitted, waiting, active, finished, steps, step_reruns;
+    uint64_t arena_bytes, arena_used, arena_peak;   /* per-query state and result buffers           */
+    uint64_t device_bytes;                          /* everything the server holds on the device     */
+    double gpu_ms;                                  /* summed device time of the steps' kernels      */
+} ps4_serve_info;
+
+/* Create a server on a context (made without PS4_F_DUMP4).  Allocates its whole budget. */
+int ps4_serve_create(ps4_ctx *ctx, const ps4_serve_config *cfg, ps4_server **out);
+void ps4_serve_destroy(ps4_server *srv);
+const char *ps4_serve_last_error(const ps4_server *srv);
+/* Queue a query; returns at once.  Tags must be unique among queries not yet taken. */
+int ps4_serve_submit_range(ps4_server *srv, uint64_t tag, uint64_t lo, uint64_t hi);
+int ps4_serve_submit_triple(ps4_server *srv, uint64_t tag, const uint64_t abc[3], uint64_t dmax);
+/* Drive the server: collect finished steps, admit waiting queries, launch the next steps.
+ * Waits up to wait_us for a query to finish; reports up to cap finished queries. */
+int ps4_serve_progress(ps4_server *srv, uint32_t wait_us, ps4_serve_done *done, uint32_t cap, uint32_t *n_done);
+/* Results of a finished query, in the layout and order of the single-query calls; the query
+ * is forgotten afterwards (PS4_ERR_OUTPUT_FULL keeps it, with the needed counts set). */
+int ps4_serve_take_range(ps4_server *srv, uint64_t tag, ps4_stats *stats, ps4_results *res);
+int ps4_serve_take_triple(ps4_server *srv, uint64_t tag, uint8_t *state, ps4_tri_ext *out, uint64_t out_cap,
+                          uint64_t *n_out, ps4_tri_stats *stats);
+void ps4_serve_get_info(const ps4_server *srv, ps4_serve_info *info);
+
 /* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
 double ps4_last_kernel_ms(const ps4_ctx *ctx);
 /* Number of kernel launches made by the last search call. */

@@ -174,7 +174,8 @@ extern "C" int ps4_create(const ps4_config *cfg, ps4_ctx **out) {
     return PS4_OK;
 }
 
-static void stats_add(ps4_stats *s, const unsigned long long *k) {
+namespace ps4 {
+void stats_add(ps4_stats *s, const unsigned long long *k) {
     uint64_t *add = &s->S_done;          // S_done .. ext_sqrt are contiguous
     for (int i = 0; i < 10; i++) add[i] += k[i];
     for (int i = 0; i < 100; i++) s->hist5[i] += k[K_HIST5 + i];
@@ -183,7 +184,7 @@ static void stats_add(ps4_stats *s, const unsigned long long *k) {
     s->max_extensions = std::max<uint64_t>(s->max_extensions, k[K_MAX_EXT]);
 }
 
-static const char *fatal_text(unsigned code) {
+const char *fatal_text(unsigned code) {
     switch (code) {
         case E_CAP_REPS: return "representation capacity exceeded";
         case E_CAP_DIVS: return "divisor capacity exceeded";
@@ -193,14 +194,50 @@ static const char *fatal_text(unsigned code) {
     }
 }
 
-// ---- one search = enqueue (host prep + launch, no wait) + finish (wait, check, collect) ----
-
 // 4-sets per S grow slowly with S (0.13 below 1e10, 0.29 near 2e12); a batch of the
 // two-kernel pipeline is sized so that this bound, with margin, fills at most 90 % of the queue.
-static double jobs_per_S_bound(uint64_t S_hi) {
+double jobs_per_S_bound(uint64_t S_hi) {
     const double dec = S_hi > 1000000000ull ? std::log10((double)S_hi / 1e9) : 0.0;
     return 0.25 + 0.05 * dec;
 }
+
+// Hits in a deterministic order -- item, S, then the reference's emission order (px, py, pz,
+// class) -- with each hit's extensions moved behind it and 6-set records re-pointed and sorted.
+void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std::vector<ps4_six> &sixes) {
+    std::vector<uint32_t> perm(hits.size());
+    for (uint32_t i = 0; i < perm.size(); i++) perm[i] = i;
+    std::sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
+        const ps4_hit &hp = hits[x], &hq = hits[y];
+        if (hp.item != hq.item) return hp.item < hq.item;
+        if (hp.S != hq.S) return hp.S < hq.S;
+        for (int i = 0; i < 4; i++)
+            if (hp.order[i] != hq.order[i]) return hp.order[i] < hq.order[i];
+        return false;
+    });
+    std::vector<ps4_hit> h2(hits.size());
+    std::vector<ps4_ext> e2;
+    e2.reserve(exts.size());
+    std::vector<uint32_t> newpos(hits.size());
+    for (uint32_t i = 0; i < perm.size(); i++) {
+        ps4_hit h = hits[perm[i]];
+        newpos[perm[i]] = i;
+        const uint32_t first = (uint32_t)e2.size();
+        for (uint32_t t = 0; t < h.n_ext; t++) e2.push_back(exts[h.first_ext + t]);
+        h.first_ext = first;
+        h2[i] = h;
+    }
+    for (auto &s6 : sixes) s6.hit = newpos[s6.hit];
+    std::sort(sixes.begin(), sixes.end(), [](const ps4_six &x, const ps4_six &y) {
+        if (x.hit != y.hit) return x.hit < y.hit;
+        if (x.t != y.t) return x.t < y.t;
+        return x.s < y.s;
+    });
+    hits.swap(h2);
+    exts.swap(e2);
+}
+}  // namespace ps4
+
+// ---- one search = enqueue (host prep + launch, no wait) + finish (wait, check, collect) ----
 
 static int enqueue_items(ps4_ctx *c) {
     PendingSearch &p = c->pend;
@@ -450,17 +487,6 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
                         st.n_exts * sizeof(ps4_ext) + st.n_sixes * sizeof(ps4_six) +
                         ((res && p.dump) ? st.n_quads * sizeof(ps4_quad) : 0);
         if (res) {
-            // deterministic order: item, S, then the reference's emission order (px, py, pz, class)
-            std::vector<uint32_t> perm(hits.size());
-            for (uint32_t i = 0; i < perm.size(); i++) perm[i] = i;
-            std::sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
-                const ps4_hit &hp = hits[x], &hq = hits[y];
-                if (hp.item != hq.item) return hp.item < hq.item;
-                if (hp.S != hq.S) return hp.S < hq.S;
-                for (int i = 0; i < 4; i++)
-                    if (hp.order[i] != hq.order[i]) return hp.order[i] < hq.order[i];
-                return false;
-            });
             res->n_hits = hits.size();
             res->n_exts = exts.size();
             res->n_sixes = sixes.size();
@@ -470,24 +496,10 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
                                (unsigned long long)res->n_hits, (unsigned long long)res->n_exts,
                                (unsigned long long)res->n_sixes);
             }
-            std::vector<uint32_t> newpos(hits.size());
-            uint32_t e = 0;
-            for (uint32_t i = 0; i < perm.size(); i++) {
-                ps4_hit h = hits[perm[i]];
-                newpos[perm[i]] = i;
-                for (uint32_t t = 0; t < h.n_ext; t++) res->exts[e + t] = exts[h.first_ext + t];
-                h.first_ext = e;
-                e += h.n_ext;
-                res->hits[i] = h;
-            }
-            std::vector<ps4_six> sx = sixes;
-            for (auto &s6 : sx) s6.hit = newpos[s6.hit];
-            std::sort(sx.begin(), sx.end(), [](const ps4_six &x, const ps4_six &y) {
-                if (x.hit != y.hit) return x.hit < y.hit;
-                if (x.t != y.t) return x.t < y.t;
-                return x.s < y.s;
-            });
-            for (size_t i = 0; i < sx.size(); i++) res->sixes[i] = sx[i];
+            canonical_order(hits, exts, sixes);
+            if (!hits.empty()) memcpy(res->hits, hits.data(), hits.size() * sizeof(ps4_hit));
+            if (!exts.empty()) memcpy(res->exts, exts.data(), exts.size() * sizeof(ps4_ext));
+            if (!sixes.empty()) memcpy(res->sixes, sixes.data(), sixes.size() * sizeof(ps4_six));
         }
         if (stats)
             for (uint32_t i = 0; i < n_items; i++) stats_add(&stats[i], &k[(size_t)i * K_SLOTS]);
@@ -561,6 +573,7 @@ extern "C" int ps4_extend_triples(ps4_ctx *c, const uint64_t *abc, uint32_t n, u
         t.out = c->d_tri_out; t.out_cap = c->tri_out_cap;
         t.n_out = c->d_tri_cnt; t.n_cand = c->d_tri_cnt + 1; t.n_sqrt = c->d_tri_cnt + 2;
         t.item_base = 0;
+        t.cand_per = t.sqrt_per = nullptr;
         CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
         CUDA_TRY(c, (cudaError_t)launch_triples(t, c->stream));
         CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));

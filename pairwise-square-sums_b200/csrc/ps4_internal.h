@@ -3,6 +3,8 @@
 #pragma once
 #include <stdint.h>
 
+#include <vector>
+
 #include "../../include/ps4.h"
 
 namespace ps4 {
@@ -89,10 +91,18 @@ struct TriArgs {
     unsigned long long *n_cand;    // same-parity complementary divisor pairs of the chosen differences
     unsigned long long *n_sqrt;    // exact square tests of d + C
     uint32_t item_base;            // added to the triple index in the records
+    unsigned long long *cand_per;  // optional (may be null): ext_cand of each triple
+    unsigned long long *sqrt_per;  // optional (may be null): ext_sqrt of each triple
 };
 enum { TRI_OK = 0, TRI_INVALID = 1, TRI_RANGE = 2 };
 
-// Read-only view of a context (ps4_api.cu), for the allocation-free entry point.
+// Host helpers shared by the single-query calls and the server (ps4_api.cu).
+void stats_add(ps4_stats *s, const unsigned long long *k);      // fold one counter block into stats (+=)
+const char *fatal_text(unsigned code);                            // the reference's FATAL message text
+double jobs_per_S_bound(uint64_t S_hi);                           // 4-set job queue entries per S, bound
+void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std::vector<ps4_six> &sixes);
+
+// Read-only view of a context (ps4_api.cu), for the allocation-free entry point and the server.
 struct CtxView {
     const uint64_t *spfq;
     const uint16_t *ndiv;

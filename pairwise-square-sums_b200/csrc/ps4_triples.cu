@@ -43,7 +43,10 @@ __global__ void __launch_bounds__(TBS) extend_triples_kernel(const TriArgs t) {
             if (r01 * r01 != m[0] + m[1] || r02 * r02 != m[0] + m[2] || r12 * r12 != m[1] + m[2]) st = TRI_INVALID;
             else if (r12 + r02 >= t.tab_n) st = TRI_RANGE;
         }
-        if (lane == 0) t.state[i] = (uint8_t)st;
+        if (lane == 0) {
+            t.state[i] = (uint8_t)st;
+            if (st != TRI_OK && t.cand_per) { t.cand_per[i] = 0; t.sqrt_per[i] = 0; }
+        }
         if (st != TRI_OK) continue;
 
         // the three differences A - B with third member C; roots ra = r_AC > rb = r_BC
@@ -80,7 +83,8 @@ __global__ void __launch_bounds__(TBS) extend_triples_kernel(const TriArgs t) {
             ndo *= (uint64_t)ex[j] + 1;
         }
         // same-parity complementary pairs f < g, the reference's ext_cand (s4.c:191)
-        if (lane == 0) cand += has2 ? ((uint64_t)(E2 - 1) * ndo) >> 1 : ndo >> 1;
+        const ull tcand = has2 ? ((uint64_t)(E2 - 1) * ndo) >> 1 : ndo >> 1;
+        if (lane == 0) cand += tcand;
 
         const int64_t dC = (int64_t)C - (int64_t)A;            // e + C = u^2 + (C - A)
         const uint32_t a64 = (uint32_t)dC & 63u;
@@ -93,53 +97,59 @@ __global__ void __launch_bounds__(TBS) extend_triples_kernel(const TriArgs t) {
         const uint64_t total = ((ndo + 1) >> 1) * W2;
         const uint64_t run = (total + 31) >> 5;
         const uint64_t x0 = (uint64_t)lane * run, x1 = min(total, x0 + run);
-        if (x0 >= x1) continue;
-        uint64_t todd = x0 / W2;
-        int d2 = dlo + (int)(x0 - todd * W2);
-        uint8_t dig[MAXP];
-        uint64_t fo = 1, go = Dodd;
-        {
-            uint64_t x = todd;
-            for (int j = j0; j < np; j++) {                       // mixed radix, first prime fastest
-                const uint64_t rdx = (uint64_t)ex[j] + 1, q = x / rdx;
-                dig[j] = (uint8_t)(x - q * rdx);
-                x = q;
-                for (int e = 0; e < dig[j]; e++) { fo *= pr[j]; go *= qinv[j]; }
+        const ull sqrt0 = nsqrt;
+        if (x0 < x1) {
+            uint64_t todd = x0 / W2;
+            int d2 = dlo + (int)(x0 - todd * W2);
+            uint8_t dig[MAXP];
+            uint64_t fo = 1, go = Dodd;
+            {
+                uint64_t x = todd;
+                for (int j = j0; j < np; j++) {                       // mixed radix, first prime fastest
+                    const uint64_t rdx = (uint64_t)ex[j] + 1, q = x / rdx;
+                    dig[j] = (uint8_t)(x - q * rdx);
+                    x = q;
+                    for (int e = 0; e < dig[j]; e++) { fo *= pr[j]; go *= qinv[j]; }
+                }
             }
-        }
-        for (uint64_t x = x0; x < x1; x++) {
-            const bool mid = (2 * todd + 1 == ndo);              // self-complementary odd part
-            if (!(mid && 2 * d2 >= E2)) {
-                const uint64_t f = fo << d2, g = go << (E2 - d2);
-                const uint64_t u = (f + g) >> 1;
-                if (u > uA && u <= umax) {
-                    const uint32_t w64 = (uint32_t)u & 63u, w63 = (uint32_t)(u % 63), w65 = (uint32_t)(u % 65);
-                    if (((QR64 >> ((w64 * w64 + a64) & 63u)) & 1) && ((QR63 >> ((w63 * w63 + a63) % 63u)) & 1) &&
-                        qr65((w65 * w65 + a65) % 65u)) {
-                        const uint64_t e = u * u - A;             // 0 < e <= dmax
-                        if (e != A && e != B && e != C) {
-                            nsqrt++;
-                            if (is_square_fast((u128)(e + C))) {
-                                const unsigned long long slot = atomicAdd(t.n_out, 1ull);
-                                if (slot < t.out_cap) {
-                                    ps4_tri_ext rec;
-                                    rec.d = e; rec.item = t.item_base + (uint32_t)i; rec.reserved = 0;
-                                    t.out[slot] = rec;
+            for (uint64_t x = x0; x < x1; x++) {
+                const bool mid = (2 * todd + 1 == ndo);              // self-complementary odd part
+                if (!(mid && 2 * d2 >= E2)) {
+                    const uint64_t f = fo << d2, g = go << (E2 - d2);
+                    const uint64_t u = (f + g) >> 1;
+                    if (u > uA && u <= umax) {
+                        const uint32_t w64 = (uint32_t)u & 63u, w63 = (uint32_t)(u % 63), w65 = (uint32_t)(u % 65);
+                        if (((QR64 >> ((w64 * w64 + a64) & 63u)) & 1) && ((QR63 >> ((w63 * w63 + a63) % 63u)) & 1) &&
+                            qr65((w65 * w65 + a65) % 65u)) {
+                            const uint64_t e = u * u - A;             // 0 < e <= dmax
+                            if (e != A && e != B && e != C) {
+                                nsqrt++;
+                                if (is_square_fast((u128)(e + C))) {
+                                    const unsigned long long slot = atomicAdd(t.n_out, 1ull);
+                                    if (slot < t.out_cap) {
+                                        ps4_tri_ext rec;
+                                        rec.d = e; rec.item = t.item_base + (uint32_t)i; rec.reserved = 0;
+                                        t.out[slot] = rec;
+                                    }
                                 }
                             }
                         }
                     }
                 }
-            }
-            if (++d2 > dhi) {
-                d2 = dlo;
-                todd++;
-                for (int j = j0; j < np; j++) {                   // odometer over the odd primes
-                    if (dig[j] < ex[j]) { dig[j]++; fo *= pr[j]; go *= qinv[j]; break; }
-                    for (int e = 0; e < dig[j]; e++) { fo *= qinv[j]; go *= pr[j]; }
-                    dig[j] = 0;
+                if (++d2 > dhi) {
+                    d2 = dlo;
+                    todd++;
+                    for (int j = j0; j < np; j++) {                   // odometer over the odd primes
+                        if (dig[j] < ex[j]) { dig[j]++; fo *= pr[j]; go *= qinv[j]; break; }
+                        for (int e = 0; e < dig[j]; e++) { fo *= qinv[j]; go *= pr[j]; }
+                        dig[j] = 0;
+                    }
                 }
             }
+        }
+        if (t.cand_per) {                                         // per-triple counters (serving)
+            const ull ts = warp_sum(nsqrt - sqrt0);
+            if (lane == 0) { t.cand_per[i] = tcand; t.sqrt_per[i] = ts; }
         }
     }
     cand = warp_sum(cand);
