@@ -63,7 +63,15 @@ typedef struct {
     uint32_t log2_tile;    /* S values per tile = 2^log2_tile (12..14); 0 = autotuned/default        */
     uint32_t ctas_per_sm;  /* resident CTAs per SM for the persistent kernel; 0 = default            */
     void *stream;          /* cudaStream_t to launch on; NULL = a stream owned by the context        */
+    uint32_t use_graph;    /* PS4_GRAPH_*: run a call's launch sequence as one captured CUDA graph   */
+    uint32_t reserved;
 } ps4_config;
+
+enum {
+    PS4_GRAPH_AUTO = 0,    /* graph for batched calls of two or more batches (default)               */
+    PS4_GRAPH_ALWAYS = 1,
+    PS4_GRAPH_NEVER = 2
+};
 
 /* Counters, identical in meaning to the reference's stats_t (exhaustive/s4.c:80-91). */
 typedef struct {
@@ -263,6 +271,31 @@ int ps4_serve_take_range(ps4_server *srv, uint64_t tag, ps4_stats *stats, ps4_re
 int ps4_serve_take_triple(ps4_server *srv, uint64_t tag, uint8_t *state, ps4_tri_ext *out, uint64_t out_cap,
                           uint64_t *n_out, ps4_tri_stats *stats);
 void ps4_serve_get_info(const ps4_server *srv, ps4_serve_info *info);
+
+/* ---- autotuning of the batched search ----
+ *
+ * Launch shape of the two-kernel pipeline: S per tile, resident tile-kernel CTAs per SM,
+ * resident engine CTAs per SM, and the largest job queue (entries, a power of two; one batch
+ * of the search fills at most 90 % of it).  No counterpart in the reference (its engine has
+ * fixed compile-time sizes, s4.c:46-52). */
+typedef struct {
+    uint32_t log2_tile;       /* 12 .. 14                                                            */
+    uint32_t gen_ctas;        /* 1 .. 2                                                              */
+    uint32_t ext_ctas;        /* 1 .. 3                                                              */
+    uint32_t log2_jobs;       /* 20 .. 27                                                            */
+    double rate;              /* S/s the tuner measured for this shape (0 if set by hand)            */
+} ps4_tuning;
+
+/* Time candidate shapes on a sample of the given workload (a slice of each of up to 8 items
+ * spread over its S span, about 2e8 S in all) and keep the fastest on the context; *best
+ * (may be NULL) receives it.  Runs for roughly budget_s seconds (0 = 2).  Results of later
+ * calls do not depend on the shape. */
+int ps4_autotune(ps4_ctx *ctx, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, double budget_s,
+                 ps4_tuning *best);
+int ps4_set_tuning(ps4_ctx *ctx, const ps4_tuning *t);
+void ps4_get_tuning(const ps4_ctx *ctx, ps4_tuning *t);
+/* CUDA-graph use of the context so far: graphs captured, graph replays. */
+void ps4_graph_counts(const ps4_ctx *ctx, uint64_t *captures, uint64_t *replays);
 
 /* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
 double ps4_last_kernel_ms(const ps4_ctx *ctx);

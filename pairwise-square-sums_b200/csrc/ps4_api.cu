@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <string>
 #include <vector>
 
@@ -55,6 +56,15 @@ struct ps4_ctx {
     uint32_t batch_div = 1;              // narrows the batches after a queue overflow
     bool fused_fallback = false;         // this call re-runs on the fused kernel (engine list overflow)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
+    // tuning (ps4_autotune / ps4_set_tuning)
+    uint32_t gen_ctas = 2, ext_ctas = 3;     // resident CTAs per SM of the tile kernel / the engine
+    uint64_t jobs_cap_max = 1ull << 27;      // largest job queue (entries)
+    double tuned_rate = 0.0;
+    // pinned staging of the segments, and the kept CUDA graph of a multi-batch call
+    Item *h_segs = nullptr; uint64_t h_segs_cap = 0;
+    cudaGraphExec_t graph_exec = nullptr;
+    std::string graph_key;
+    uint64_t graph_launches = 0, graph_captures = 0, graph_replays = 0;
     // triple extension (grown on demand)
     uint64_t *d_tri_in = nullptr; uint64_t tri_in_cap = 0;
     uint8_t *d_tri_state = nullptr; uint64_t tri_state_cap = 0;
@@ -121,6 +131,8 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     cudaFree(c->d_scratch); cudaFree(c->d_status); cudaFree(c->d_jobs);
     cudaFree(c->d_tri_in); cudaFree(c->d_tri_state); cudaFree(c->d_tri_out); cudaFree(c->d_tri_cnt);
     if (c->h_status) cudaFreeHost(c->h_status);
+    if (c->h_segs) cudaFreeHost(c->h_segs);
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -239,49 +251,71 @@ void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std
 
 // ---- one search = enqueue (host prep + launch, no wait) + finish (wait, check, collect) ----
 
+// Cut a call's items into batches for the two-kernel pipeline: each batch holds at most
+// ~90 % of the job queue in expected 4-sets (jobs_per_S_bound).  Within a batch the segments
+// are ordered by estimated cost per tile, ascending; the tile kernels claim tiles from the
+// last one down (tile_bounds), so the costliest tiles -- the highest S, whose representation
+// and 4-set counts are largest -- start first and narrow partial tiles fill the tail.
+static void plan_batches(ps4_ctx *c, const std::vector<Item> &items, unsigned TL, std::vector<Item> &segs,
+                         std::vector<size_t> &batch_start, std::vector<uint64_t> &batch_tiles) {
+    const uint32_t n_items = (uint32_t)items.size();
+    size_t i = 0;
+    uint64_t pos = n_items ? items[0].lo : 0;
+    while (i < n_items) {
+        const size_t b0 = segs.size();
+        double budget = 0.9 * (double)c->jobs_cap / (double)c->batch_div;
+        while (i < n_items && budget > 0) {
+            const Item &it = items[i];
+            if (pos < it.lo) pos = it.lo;
+            const double dens = jobs_per_S_bound(it.hi);
+            uint64_t room = (uint64_t)(budget / dens);
+            room = std::max<uint64_t>(room >> TL, 1) << TL;          // whole tiles
+            const uint64_t end = it.hi - pos > room ? pos + room : it.hi;
+            if (end > pos) {
+                Item sg;
+                sg.lo = pos; sg.hi = end; sg.id = it.id; sg.pad = 0; sg.tile_base = 0;
+                segs.push_back(sg);
+            }
+            budget -= dens * (double)(end - pos);
+            pos = end;
+            if (pos >= it.hi) { i++; if (i < n_items) pos = items[i].lo; }
+        }
+        if (segs.size() == b0) continue;
+        std::stable_sort(segs.begin() + b0, segs.end(), [](const Item &x, const Item &y) {
+            if (x.hi != y.hi) return x.hi < y.hi;               // cost density grows with S
+            return x.hi - x.lo < y.hi - y.lo;
+        });
+        uint64_t tiles = 0;
+        for (size_t k = b0; k < segs.size(); k++) {
+            segs[k].tile_base = tiles;
+            tiles += (segs[k].hi - segs[k].lo + (1ull << TL) - 1) >> TL;
+        }
+        batch_start.push_back(b0);
+        batch_tiles.push_back(tiles);
+    }
+}
+
+template <class T>
+static void key_add(std::string &k, const T &v) {
+    k.append(reinterpret_cast<const char *>(&v), sizeof v);
+}
+
 static int enqueue_items(ps4_ctx *c) {
     PendingSearch &p = c->pend;
     const uint32_t n_items = (uint32_t)p.items.size();
     const unsigned TL = c->tile_log2;
     const int kernel = c->fused_fallback ? (int)PS4_KERNEL_FUSED : (int)c->cfg.kernel;
-    if (kernel == PS4_KERNEL_BATCHED) {          // queue: the call's expected 4-sets, 2^20 .. 2^27
+    if (kernel == PS4_KERNEL_BATCHED) {          // queue: the call's expected 4-sets, 2^20 .. jobs_cap_max
         double need = 0;
         for (uint32_t i = 0; i < n_items; i++)
             need += jobs_per_S_bound(p.items[i].hi) * (double)(p.items[i].hi - p.items[i].lo);
-        while (c->jobs_cap < (1ull << 27) && (double)c->jobs_cap * 0.9 < need) c->jobs_cap <<= 1;
+        while (c->jobs_cap < c->jobs_cap_max && (double)c->jobs_cap * 0.9 < need) c->jobs_cap <<= 1;
     }
     std::vector<Item> segs;                      // all batches' segments, batch after batch
     std::vector<size_t> batch_start;             // segs index where each batch begins
     std::vector<uint64_t> batch_tiles;
     if (kernel == PS4_KERNEL_BATCHED) {
-        // cut the items into batches of at most ~90 % of the job queue in expected 4-sets
-        size_t i = 0;
-        uint64_t pos = n_items ? p.items[0].lo : 0;
-        while (i < n_items) {
-            batch_start.push_back(segs.size());
-            double budget = 0.9 * (double)c->jobs_cap / (double)c->batch_div;
-            uint64_t tiles = 0;
-            while (i < n_items && budget > 0) {
-                const Item &it = p.items[i];
-                if (pos < it.lo) pos = it.lo;
-                const double dens = jobs_per_S_bound(it.hi);
-                uint64_t room = (uint64_t)(budget / dens);
-                room = std::max<uint64_t>(room >> TL, 1) << TL;          // whole tiles
-                const uint64_t end = it.hi - pos > room ? pos + room : it.hi;
-                if (end > pos) {
-                    Item sg;
-                    sg.lo = pos; sg.hi = end; sg.id = it.id; sg.pad = 0;
-                    sg.tile_base = tiles;
-                    tiles += (end - pos + (1ull << TL) - 1) >> TL;
-                    segs.push_back(sg);
-                }
-                budget -= dens * (double)(end - pos);
-                pos = end;
-                if (pos >= it.hi) { i++; if (i < n_items) pos = p.items[i].lo; }
-            }
-            if (segs.size() == batch_start.back()) batch_start.pop_back();
-            else batch_tiles.push_back(tiles);
-        }
+        plan_batches(c, p.items, TL, segs, batch_start, batch_tiles);
     } else {
         uint64_t tiles = 0;
         for (uint32_t i = 0; i < n_items; i++) {
@@ -300,13 +334,26 @@ static int enqueue_items(ps4_ctx *c) {
         tiles_total += t;
     }
     p.tiles = tiles_total;
+
+    // every allocation before any launch (a captured call may allocate nothing)
     if (grow32(c, c->d_items, c->items_cap, std::max<size_t>(segs.size(), 1))) return PS4_ERR_CUDA;
-    if (!segs.empty())
-        CUDA_TRY(c, cudaMemcpyAsync(c->d_items, segs.data(), segs.size() * sizeof(Item), cudaMemcpyHostToDevice,
-                                    c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long), c->stream));
-    CUDA_TRY(c, cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream));
-    c->h2d_bytes += segs.size() * sizeof(Item);
+    if (c->h_segs_cap < segs.size() || !c->h_segs) {
+        if (c->h_segs) cudaFreeHost(c->h_segs);
+        c->h_segs = nullptr;
+        c->h_segs_cap = std::max<uint64_t>(segs.size(), 1024);
+        CUDA_TRY(c, cudaMallocHost((void **)&c->h_segs, c->h_segs_cap * sizeof(Item)));
+    }
+    if (kernel == PS4_KERNEL_BATCHED && c->d_jobs_words < 6 * c->jobs_cap)
+        if (grow(c, c->d_jobs, c->d_jobs_words, 6 * c->jobs_cap)) return PS4_ERR_CUDA;
+    const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
+    int grid = c->num_sms * (c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1);
+    if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
+    if (kernel == PS4_KERNEL_FUSED) {
+        uint64_t cap = c->scratch_words;
+        if (grow(c, c->d_scratch, cap, (uint64_t)grid * 6 * stage_cap)) return PS4_ERR_CUDA;
+        c->scratch_words = cap;
+    }
+
     SearchArgs a;
     memset(&a, 0, sizeof a);
     a.log2_tile = TL;
@@ -319,45 +366,85 @@ static int enqueue_items(ps4_ctx *c) {
     a.status = c->d_status;
     a.cap_reps = c->cfg.cap_reps; a.cap_divs = c->cfg.cap_divs; a.cap_ext = c->cfg.cap_ext;
     a.flags = c->cfg.flags & (p.dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
+    a.jobs = c->d_jobs;
+    a.jobs_cap = c->jobs_cap;
+    const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
+    const int g_gen = c->num_sms * (int)c->gen_ctas, g_ext = c->num_sms * (int)c->ext_ctas;
+
+    // A call of several batches runs as one CUDA graph holding its whole launch sequence; the
+    // graph is kept and replayed while the next call is the same (items, sizes, buffers).
+    const bool graph = c->cfg.use_graph == PS4_GRAPH_ALWAYS ||
+                       (c->cfg.use_graph == PS4_GRAPH_AUTO && kernel == PS4_KERNEL_BATCHED && batch_start.size() >= 2);
+    std::string key;
+    if (graph) {
+        key.append(reinterpret_cast<const char *>(segs.data()), segs.size() * sizeof(Item));
+        for (size_t b : batch_start) key_add(key, b);
+        key_add(key, a);
+        key_add(key, kernel); key_add(key, n_items); key_add(key, grid); key_add(key, g_gen); key_add(key, g_ext);
+        key_add(key, stage_cap); key_add(key, c->d_scratch); key_add(key, c->h_segs); key_add(key, c->d_items);
+        key_add(key, c->stream);
+    }
+    if (!segs.empty()) memcpy(c->h_segs, segs.data(), segs.size() * sizeof(Item));
+    c->h2d_bytes += segs.size() * sizeof(Item);
     CUDA_TRY(c, cudaEventRecord(c->ev0, c->stream));
-    if (kernel == PS4_KERNEL_BATCHED) {
-        if (c->d_jobs_words < 6 * c->jobs_cap) {
-            if (grow(c, c->d_jobs, c->d_jobs_words, 6 * c->jobs_cap)) return PS4_ERR_CUDA;
-        }
-        a.jobs = c->d_jobs;
-        a.jobs_cap = c->jobs_cap;
-        const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
-        for (size_t b = 0; b < batch_start.size(); b++) {
-            const size_t s0 = batch_start[b], s1 = b + 1 < batch_start.size() ? batch_start[b + 1] : segs.size();
-            a.items = c->d_items + s0;
-            a.n_items = (uint32_t)(s1 - s0);
-            a.n_tiles = batch_tiles[b];
-            const int g = (int)std::min<uint64_t>((uint64_t)gen_grid(c->num_sms), std::max<uint64_t>(a.n_tiles, 1));
-            // n_jobs, tile_next, ext_next: the per-batch tail of the status block
-            CUDA_TRY(c, cudaMemsetAsync(&c->d_status->n_jobs, 0, 2 * sizeof(unsigned long long), c->stream));
-            CUDA_TRY(c, (cudaError_t)launch_gen(a, g, c->stream));
-            c->last_launches++;
-            if (ext) {
-                CUDA_TRY(c, (cudaError_t)launch_ext(a, ext_grid(c->num_sms), c->stream));
+    if (graph && c->graph_exec && key == c->graph_key) {
+        CUDA_TRY(c, cudaGraphLaunch(c->graph_exec, c->stream));
+        c->last_launches += c->graph_launches;
+        c->graph_replays++;
+    } else {
+        if (graph) CUDA_TRY(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+        const uint64_t launches0 = c->last_launches;
+        int rc = PS4_OK;
+        cudaError_t e = cudaSuccess;
+        if (!segs.empty())
+            e = cudaMemcpyAsync(c->d_items, c->h_segs, segs.size() * sizeof(Item), cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(c->d_counters, 0, (size_t)n_items * K_SLOTS * sizeof(unsigned long long), c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->d_status, 0, sizeof(Status), c->stream);
+        if (e == cudaSuccess && kernel == PS4_KERNEL_BATCHED) {
+            for (size_t b = 0; b < batch_start.size() && e == cudaSuccess; b++) {
+                const size_t s0 = batch_start[b], s1 = b + 1 < batch_start.size() ? batch_start[b + 1] : segs.size();
+                a.items = c->d_items + s0;
+                a.n_items = (uint32_t)(s1 - s0);
+                a.n_tiles = batch_tiles[b];
+                const int g = (int)std::min<uint64_t>((uint64_t)g_gen, std::max<uint64_t>(a.n_tiles, 1));
+                // n_jobs, tile_next, ext_next: the per-batch tail of the status block
+                e = cudaMemsetAsync(&c->d_status->n_jobs, 0, 2 * sizeof(unsigned long long), c->stream);
+                if (e == cudaSuccess) e = (cudaError_t)launch_gen(a, g, c->stream);
                 c->last_launches++;
+                if (e == cudaSuccess && ext) {
+                    e = (cudaError_t)launch_ext(a, g_ext, c->stream);
+                    c->last_launches++;
+                }
+            }
+        } else if (e == cudaSuccess && tiles_total > 0) {
+            a.items = c->d_items; a.n_items = (uint32_t)segs.size(); a.n_tiles = tiles_total;
+            a.scratch = c->d_scratch; a.stage_cap = stage_cap;
+            // launch_search's selector: PS4_KERNEL_BATCHED there is the fused persistent kernel
+            e = (cudaError_t)launch_search(a, kernel == PS4_KERNEL_PLAIN ? PS4_KERNEL_PLAIN : PS4_KERNEL_BATCHED, grid,
+                                           c->stream);
+            c->last_launches++;
+        }
+        if (graph) {
+            cudaGraph_t g = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+            if (e == cudaSuccess) e = e2;
+            if (e == cudaSuccess) {
+                if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+                c->graph_exec = nullptr;
+                c->graph_key.clear();
+                e = cudaGraphInstantiate(&c->graph_exec, g, 0);
+            }
+            if (g) cudaGraphDestroy(g);
+            if (e == cudaSuccess) e = cudaGraphLaunch(c->graph_exec, c->stream);
+            if (e == cudaSuccess) {
+                c->graph_key.swap(key);
+                c->graph_launches = c->last_launches - launches0;
+                c->graph_captures++;
             }
         }
-    } else if (tiles_total > 0) {
-        const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
-        int ctas_per_sm = c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1;
-        int grid = c->num_sms * ctas_per_sm;
-        if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
-        if (kernel == PS4_KERNEL_FUSED) {
-            uint64_t cap = c->scratch_words;
-            if (grow(c, c->d_scratch, cap, (uint64_t)grid * 6 * stage_cap)) return PS4_ERR_CUDA;
-            c->scratch_words = cap;
-        }
-        a.items = c->d_items; a.n_items = (uint32_t)segs.size(); a.n_tiles = tiles_total;
-        a.scratch = c->d_scratch; a.stage_cap = stage_cap;
-        // launch_search's selector: PS4_KERNEL_BATCHED there is the fused persistent kernel
-        CUDA_TRY(c, (cudaError_t)launch_search(a, kernel == PS4_KERNEL_PLAIN ? PS4_KERNEL_PLAIN : PS4_KERNEL_BATCHED,
-                                               grid, c->stream));
-        c->last_launches++;
+        if (e != cudaSuccess) rc = set_err(c, PS4_ERR_CUDA, "search launch failed: %s", cudaGetErrorString(e));
+        if (rc) return rc;
     }
     CUDA_TRY(c, cudaEventRecord(c->ev1, c->stream));
     CUDA_TRY(c, cudaMemcpyAsync(c->h_status, c->d_status, sizeof(Status), cudaMemcpyDeviceToHost, c->stream));
@@ -387,8 +474,15 @@ static int begin_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint3
     if (grow32(c, c->d_counters, c->counters_items, (uint64_t)n_items * K_SLOTS)) return PS4_ERR_CUDA;
     p.dump = (c->cfg.flags & PS4_F_DUMP4) && want_dump && dump_cap > 0;
     if (p.dump && grow(c, c->d_quads, c->quads_cap, dump_cap)) return PS4_ERR_CUDA;
-    if (grow32(c, c->d_hits, c->hits_cap, std::max<uint32_t>(c->hits_cap, 1u << 16))) return PS4_ERR_CUDA;
-    if (grow32(c, c->d_exts, c->exts_cap, std::max<uint32_t>(c->exts_cap, 1u << 17))) return PS4_ERR_CUDA;
+    // result buffers sized up front from the call's width (4-sets with an extension stay below
+    // 1.5e-5 per S on every checked range), so a long call is not repeated to grow them
+    double width = 0;
+    for (uint32_t i = 0; i < n_items; i++) width += (double)(p.items[i].hi - p.items[i].lo);
+    const uint64_t hits_est = std::min<uint64_t>(1024 + (uint64_t)(2e-5 * width), 1ull << 30);
+    if (grow32(c, c->d_hits, c->hits_cap, std::max<uint64_t>({(uint64_t)c->hits_cap, 1u << 16, hits_est})))
+        return PS4_ERR_CUDA;
+    if (grow32(c, c->d_exts, c->exts_cap, std::max<uint64_t>({(uint64_t)c->exts_cap, 1u << 17, 2 * hits_est})))
+        return PS4_ERR_CUDA;
     if (grow32(c, c->d_sixes, c->sixes_cap, std::max<uint32_t>(c->sixes_cap, 1024))) return PS4_ERR_CUDA;
     int rc = enqueue_items(c);
     if (rc == PS4_OK) p.active = true;
@@ -541,6 +635,101 @@ extern "C" int ps4_search_finish(ps4_ctx *c, ps4_stats *stats, ps4_results *res)
 extern "C" void ps4_last_transfer_bytes(const ps4_ctx *c, uint64_t *h2d, uint64_t *d2h) {
     if (h2d) *h2d = c ? c->h2d_bytes : 0;
     if (d2h) *d2h = c ? c->d2h_bytes : 0;
+}
+
+// ---- tuning ----
+
+extern "C" int ps4_set_tuning(ps4_ctx *c, const ps4_tuning *t) {
+    if (!c || !t) return PS4_ERR_ARG;
+    if (t->log2_tile < 12 || t->log2_tile > 14 || t->gen_ctas < 1 || t->gen_ctas > 2 || t->ext_ctas < 1 ||
+        t->ext_ctas > 3 || t->log2_jobs < 20 || t->log2_jobs > 27)
+        return set_err(c, PS4_ERR_ARG, "tuning out of range (log2_tile 12..14, gen_ctas 1..2, ext_ctas 1..3, "
+                                       "log2_jobs 20..27)");
+    c->tile_log2 = t->log2_tile;
+    c->gen_ctas = t->gen_ctas;
+    c->ext_ctas = t->ext_ctas;
+    c->jobs_cap_max = 1ull << t->log2_jobs;
+    if (c->jobs_cap > c->jobs_cap_max) c->jobs_cap = c->jobs_cap_max;
+    c->tuned_rate = t->rate;
+    return PS4_OK;
+}
+
+extern "C" void ps4_get_tuning(const ps4_ctx *c, ps4_tuning *t) {
+    if (!c || !t) return;
+    t->log2_tile = c->tile_log2;
+    t->gen_ctas = c->gen_ctas;
+    t->ext_ctas = c->ext_ctas;
+    uint32_t lj = 0;
+    while ((1ull << lj) < c->jobs_cap_max) lj++;
+    t->log2_jobs = lj;
+    t->rate = c->tuned_rate;
+}
+
+extern "C" void ps4_graph_counts(const ps4_ctx *c, uint64_t *captures, uint64_t *replays) {
+    if (captures) *captures = c ? c->graph_captures : 0;
+    if (replays) *replays = c ? c->graph_replays : 0;
+}
+
+// The tuner's sample: a slice of up to 8 items chosen at even quantiles of their start, each
+// slice centred in its item, about 2e8 S in all -- enough for every candidate shape to fill
+// the device several times over while the whole tuning stays within a few seconds.
+extern "C" int ps4_autotune(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint32_t n_items, double budget_s,
+                            ps4_tuning *best) {
+    if (!c) return PS4_ERR_ARG;
+    if (!lo || !hi || n_items == 0) return set_err(c, PS4_ERR_ARG, "ps4_autotune: empty workload");
+    if (c->cfg.kernel != PS4_KERNEL_BATCHED) return set_err(c, PS4_ERR_ARG, "ps4_autotune tunes the batched kernels");
+    if (c->pend.active) return set_err(c, PS4_ERR_ARG, "a search is enqueued on this context");
+    if (budget_s <= 0) budget_s = 2.0;
+    std::vector<uint32_t> idx(n_items);
+    for (uint32_t i = 0; i < n_items; i++) idx[i] = i;
+    std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return lo[x] < lo[y]; });
+    const uint32_t k = std::min<uint32_t>(n_items, 8);
+    const uint64_t per = (uint64_t)(2e8 / k);
+    std::vector<uint64_t> slo, shi;
+    for (uint32_t j = 0; j < k; j++) {
+        const uint32_t i = idx[(uint64_t)j * n_items / k + (n_items / k) / 2];
+        const uint64_t a = std::max<uint64_t>(lo[i], 1), b = std::max(hi[i], a);
+        const uint64_t w = std::min<uint64_t>(b - a, per);
+        const uint64_t s0 = a + ((b - a) - w) / 2;
+        if (w) { slo.push_back(s0); shi.push_back(s0 + w); }
+    }
+    if (slo.empty()) return set_err(c, PS4_ERR_ARG, "ps4_autotune: workload has no S");
+    uint64_t sample_S = 0;
+    for (size_t j = 0; j < slo.size(); j++) sample_S += shi[j] - slo[j];
+    std::vector<ps4_stats> st(slo.size());
+    ps4_tuning cur;
+    ps4_get_tuning(c, &cur);
+    const ps4_tuning start = cur;
+    ps4_tuning top = cur;
+    top.rate = 0.0;
+    struct timespec w0, w1;
+    clock_gettime(CLOCK_MONOTONIC, &w0);
+    for (uint32_t tl : {14u, 13u, 12u})
+        for (uint32_t gc : {2u, 1u})
+            for (uint32_t ec : {3u, 2u}) {
+                clock_gettime(CLOCK_MONOTONIC, &w1);
+                const double el = (double)(w1.tv_sec - w0.tv_sec) + 1e-9 * (double)(w1.tv_nsec - w0.tv_nsec);
+                if (el > budget_s && top.rate > 0) break;
+                ps4_tuning t = cur;
+                t.log2_tile = tl; t.gen_ctas = gc; t.ext_ctas = ec; t.rate = 0;
+                int rc = ps4_set_tuning(c, &t);
+                double ms = 1e300;
+                for (int rep = 0; rep < 2 && rc == PS4_OK; rep++) {
+                    rc = begin_items(c, slo.data(), shi.data(), (uint32_t)slo.size(), false, 0);
+                    if (rc == PS4_OK) rc = finish_items(c, st.data(), nullptr);
+                    c->pend.active = false;
+                    if (rc == PS4_OK && rep == 1) ms = c->last_ms;
+                }
+                if (rc != PS4_OK) {
+                    ps4_set_tuning(c, &start);
+                    return rc;
+                }
+                const double rate = (double)sample_S / (ms * 1e-3);
+                if (rate > top.rate) { top = t; top.rate = rate; }
+            }
+    ps4_set_tuning(c, &top);
+    if (best) *best = top;
+    return PS4_OK;
 }
 
 // ---- triple extension ----

@@ -32,6 +32,10 @@ PS4_KERNEL_BATCHED = 0
 PS4_KERNEL_PLAIN = 1
 PS4_KERNEL_FUSED = 2
 
+PS4_GRAPH_AUTO = 0
+PS4_GRAPH_ALWAYS = 1
+PS4_GRAPH_NEVER = 2
+
 PS4_HIT_MULTI = 1
 PS4_HIT_DRILL_OK = 2
 PS4_EXT_FIVE = 1
@@ -45,7 +49,15 @@ class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("s_hi_max", C.c_uint64), ("cap_reps", C.c_uint32),
                 ("cap_divs", C.c_uint32), ("cap_ext", C.c_uint32), ("flags", C.c_uint32),
                 ("kernel", C.c_uint32), ("log2_tile", C.c_uint32), ("ctas_per_sm", C.c_uint32),
-                ("stream", C.c_void_p)]
+                ("stream", C.c_void_p), ("use_graph", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("log2_tile", C.c_uint32), ("gen_ctas", C.c_uint32), ("ext_ctas", C.c_uint32),
+                ("log2_jobs", C.c_uint32), ("rate", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {n: getattr(self, n) for n, _ in self._fields_}
 
 
 class Stats(C.Structure):
@@ -128,6 +140,10 @@ def load() -> C.CDLL:
         "ps4_last_transfer_bytes": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
         "ps4_extend_triples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,
                                          C.c_uint64, P(C.c_uint64), P(TriStats)]),
+        "ps4_autotune": (C.c_int, [C.c_void_p, P(C.c_uint64), P(C.c_uint64), C.c_uint32, C.c_double, P(Tuning)]),
+        "ps4_set_tuning": (C.c_int, [C.c_void_p, P(Tuning)]),
+        "ps4_get_tuning": (None, [C.c_void_p, P(Tuning)]),
+        "ps4_graph_counts": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
         "ps4_format_hit": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),
         "ps4_format_six": (C.c_long, [P(Hit), P(Ext), P(Six), C.c_char_p, C.c_size_t]),
         "ps4_format_drill": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),

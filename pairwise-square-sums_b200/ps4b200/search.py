@@ -43,7 +43,8 @@ class Search:
 
     def __init__(self, s_hi_max: int, device: int = 0, *, noext: bool = False, verify: bool = False,
                  dump4: bool = False, kernel: str = "batched", cap_reps: int = 0, cap_divs: int = 0,
-                 cap_ext: int = 0, log2_tile: int = 0, ctas_per_sm: int = 0, stream: int | None = None):
+                 cap_ext: int = 0, log2_tile: int = 0, ctas_per_sm: int = 0, stream: int | None = None,
+                 graph: str = "auto"):
         self.lib = _abi.load()
         cfg = _abi.Config()
         cfg.device = device
@@ -56,6 +57,8 @@ class Search:
         cfg.log2_tile = log2_tile
         cfg.ctas_per_sm = ctas_per_sm
         cfg.stream = stream
+        cfg.use_graph = {"auto": _abi.PS4_GRAPH_AUTO, "always": _abi.PS4_GRAPH_ALWAYS,
+                         "never": _abi.PS4_GRAPH_NEVER}[graph]
         self.dump4 = dump4
         self.ctx = C.c_void_p()
         rc = self.lib.ps4_create(C.byref(cfg), C.byref(self.ctx))
@@ -116,6 +119,16 @@ class Search:
             self._quads, r.quads_cap = _alloc(_abi.Quad, r.n_quads * 3 // 2)
         self._bind()
 
+    def _reserve(self, width: int):
+        """Host result buffers for a call of this many S (as the library sizes its own)."""
+        need = 1024 + int(2e-5 * width)
+        r = self._res
+        if need > r.hits_cap:
+            self._hits, r.hits_cap = _alloc(_abi.Hit, need)
+        if 2 * need > r.exts_cap:
+            self._exts, r.exts_cap = _alloc(_abi.Ext, 2 * need)
+        self._bind()
+
     def _call(self, fn):
         while True:
             rc = fn()
@@ -128,6 +141,7 @@ class Search:
 
     def range(self, lo: int, hi: int, *, want_lines: bool = True) -> RangeResult:
         """Every S in [lo, hi): counters and result lines (one reference invocation)."""
+        self._reserve(max(hi - lo, 0))
         st = _abi.Stats()
         self._call(lambda: self.lib.ps4_search_range(self.ctx, lo, hi, C.byref(st), C.byref(self._res)))
         out = RangeResult(stats=st.as_dict(), kernel_ms=self.last_kernel_ms)
@@ -150,6 +164,32 @@ class Search:
             self._collect(out)
         return out
 
+    def autotune(self, los, his, budget_s: float = 2.0) -> dict:
+        """Time launch shapes on a sample of the workload; the fastest stays on the context."""
+        n = len(los)
+        lo_arr = (C.c_uint64 * n)(*los)
+        hi_arr = (C.c_uint64 * n)(*his)
+        t = _abi.Tuning()
+        self._call(lambda: self.lib.ps4_autotune(self.ctx, lo_arr, hi_arr, n, budget_s, C.byref(t)))
+        return t.as_dict()
+
+    @property
+    def tuning(self) -> dict:
+        t = _abi.Tuning()
+        self.lib.ps4_get_tuning(self.ctx, C.byref(t))
+        return t.as_dict()
+
+    @tuning.setter
+    def tuning(self, d: dict) -> None:
+        t = _abi.Tuning(d["log2_tile"], d["gen_ctas"], d["ext_ctas"], d["log2_jobs"], d.get("rate", 0.0))
+        self._call(lambda: self.lib.ps4_set_tuning(self.ctx, C.byref(t)))
+
+    def graph_counts(self) -> tuple[int, int]:
+        """(CUDA graphs captured, graph replays) on this context so far."""
+        a, b = C.c_uint64(), C.c_uint64()
+        self.lib.ps4_graph_counts(self.ctx, C.byref(a), C.byref(b))
+        return int(a.value), int(b.value)
+
     def transfer_bytes(self) -> tuple[int, int]:
         h2d, d2h = C.c_uint64(), C.c_uint64()
         self.lib.ps4_last_transfer_bytes(self.ctx, C.byref(h2d), C.byref(d2h))
@@ -160,6 +200,7 @@ class Search:
         n = len(los)
         lo_arr = (C.c_uint64 * n)(*los)
         hi_arr = (C.c_uint64 * n)(*his)
+        self._reserve(sum(max(int(b) - int(a), 0) for a, b in zip(los, his)))
         st = (_abi.Stats * n)()
         self._call(lambda: self.lib.ps4_search_batch(self.ctx, lo_arr, hi_arr, n, st, C.byref(self._res)))
         out = RangeResult(stats={}, kernel_ms=self.last_kernel_ms)
