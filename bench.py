@@ -163,10 +163,149 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
+# ------------------------------------------------------------------ side workloads
+
+TRIPLE_SEED = 20261203
+
+
+def measure_triples(local: int, stream, n: int = 10 ** 5, dmax: int = 10 ** 12, steps: int = 5, warmup: int = 3,
+                    cpu: bool = True) -> dict:
+    """Batched triple extension: n seeded triples (x, y, z uniform in [1, 1e5]), every d <= dmax.
+    value = triples/s of the kernel (CUDA events on the launch stream); e2e through
+    ps4_extend_triples with the triples in pinned host memory and sorted records back."""
+    import numpy as np
+    import torch
+    from ps4b200 import Search, workloads
+    abc = workloads.triples(n, seed=TRIPLE_SEED)
+    pinned = torch.empty((n, 3), dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    pinned[:] = abc
+    with Search(2 * 10 ** 12, device=local, stream=stream.cuda_stream) as s:
+        for _ in range(warmup):
+            s.extend_triples(pinned, dmax, as_lists=False)
+        torch.cuda.synchronize()
+        kms, wall, st = 0.0, 0.0, None
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            recs, state, st = s.extend_triples(pinned, dmax, as_lists=False)
+            kms += s.last_kernel_ms
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = e0.elapsed_time(e1)
+        h2d, d2h = s.transfer_bytes()
+    out = {"workload": f"{n} seeded triples (x,y,z uniform in [1,1e5]), every d <= {dmax:.0e}",
+           "value": n * steps / (kms / 1e3), "unit": "triples/s",
+           "candidates_per_s": st["ext_cand"] * steps / (kms / 1e3), "kernel_ms": kms / steps,
+           "exts": st["exts"],
+           "e2e": {"value": n * steps / (wall / 1e3), "unit": "triples/s", "h2d_bytes_per_step": h2d,
+                   "d2h_bytes_per_step": d2h}}
+    if cpu:
+        from oracle import orc
+        k = 20000
+        t0 = time.perf_counter()
+        for a, b, c in abc[:k].tolist():
+            orc.extend_triple(a, b, c, dmax)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": k / t, "unit": "triples/s", "cores": 1, "kind": "port",
+                               "sample": f"first {k} of the same triples, oracle/ps4_oracle.c orc_extend_triple"}
+    return out
+
+
+def measure_serve(local: int, n_req: int, rate: float, seed: int = 20261204, budget: int = 8 << 30) -> dict:
+    """The serving loop on a seeded Poisson stream (70 % subranges, width log-uniform in
+    [1e4, 1e9], offset uniform in [1, 1e12]; 30 % triples, d <= 1e12), replayed in real time;
+    then the same requests in the offline batched form (one batch call, one triple call),
+    with every result compared."""
+    from ps4b200 import Search, workloads
+    from ps4b200.serve import Server, run_stream
+    reqs = workloads.requests(n_req, seed=seed, rate=rate)
+    with Search(10 ** 12 + 10 ** 9 + 1, device=local) as s:
+        with Server(s, hbm_budget=budget) as srv:
+            run_stream(srv, workloads.requests(20, seed=seed + 7, rate=1000.0, wmax=1e7))     # warm-up
+            rep = run_stream(srv, reqs)
+        ranges = [r for r in reqs if r.kind == "range"]
+        tris = [r for r in reqs if r.kind == "triple"]
+        t0 = time.monotonic()
+        stats, res = s.batch([r.lo for r in ranges], [r.hi for r in ranges])
+        ext, state, tst = s.extend_triples([r.abc for r in tris], 10 ** 12)
+        off_s = time.monotonic() - t0
+    by_item = {}
+    for line, item in zip(res.lines, res.items):
+        by_item.setdefault(item, []).append(line)
+    same = True
+    for i, r in enumerate(ranges):
+        g = rep.results[r.rid]
+        same &= (not isinstance(g, Exception)) and g.lines == by_item.get(i, []) and g.stats == stats[i]
+    for i, r in enumerate(tris):
+        g = rep.results[r.rid]
+        same &= (not isinstance(g, Exception)) and g[0] == ext[i] and g[1] == int(state[i])
+    S_total = sum(r.hi - r.lo for r in ranges)
+    lat = sorted(rep.latency_s.values())
+    return {"workload": f"{n_req} requests, Poisson at {rate:g}/s, seed {seed}: 70% subranges (width "
+                        f"log-uniform [1e4,1e9], offset uniform [1,1e12]), 30% triples (d <= 1e12)",
+            "p50_ms": 1e3 * rep.percentile(50), "p90_ms": 1e3 * rep.percentile(90),
+            "p99_ms": 1e3 * rep.percentile(99), "max_ms": 1e3 * lat[-1],
+            "requests_per_s": n_req / rep.wall_s, "S_per_s": S_total / rep.wall_s, "wall_s": rep.wall_s,
+            "offline_S_per_s": S_total / off_s, "offline_s": off_s,
+            "identical_to_offline": bool(same),
+            "steps": rep.info["steps"], "step_reruns": rep.info["step_reruns"],
+            "gpu_busy_frac": rep.info["gpu_ms"] / 1e3 / rep.wall_s,
+            "hbm_budget_bytes": budget, "arena_peak_bytes": rep.info["arena_peak"]}
+
+
+def run_subranges(args, local: int):
+    """The batched uneven-subrange workload as its own line: 4096 subranges (seed 20261203,
+    widths log-uniform in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call, autotuned."""
+    import torch
+    from ps4b200 import Search, workloads
+    los, his = workloads.subranges(4096, seed=20261203)
+    los, his = los.tolist(), his.tolist()
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    props = torch.cuda.get_device_properties(local)
+    with Search(max(his) + 1, device=local, stream=stream.cuda_stream) as s:
+        tune = s.autotune(los, his, budget_s=4.0)
+        for _ in range(args.warmup):
+            s.batch(los, his, want_lines=False)
+        clocks = ClockSampler(str(getattr(props, "uuid", "")))
+        clocks.start()
+        torch.cuda.synchronize()
+        kms, launches = 0.0, 0
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            stats, _ = s.batch(los, his, want_lines=False)
+            kms += s.last_kernel_ms
+            launches += s.last_launches
+        e1.record(stream)
+        torch.cuda.synchronize()
+        clk = clocks.stop()
+        caps, replays = s.graph_counts()
+    S = sum(h - l for l, h in zip(los, his))
+    line = {"metric": METRIC, "value": S * args.steps / (kms / 1e3), "unit": UNIT, "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": kms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": {"workload": "4096 uneven subranges, seed 20261203, widths log-uniform in [1e5,1e9], "
+                                   "offsets uniform in [1,1e11], one call = one CUDA graph", "S_total": S,
+                       "tuning": tune, "graphs_captured": caps, "graph_replays": replays},
+            "candidates_per_s": sum(st["ext_cand"] for st in stats) * args.steps / (kms / 1e3),
+            "e2e": {"value": S * args.steps / (e0.elapsed_time(e1) / 1e3), "unit": UNIT},
+            "gpu_launches": launches, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(args, local: int):
+    import torch
+    torch.cuda.set_device(local)
+    out = measure_serve(local, args.serve_requests, args.serve_rate)
+    print(json.dumps({"metric": "serve_latency_p50_p99", **out}), flush=True)
+
+
 # ------------------------------------------------------------------ our arm
 
-def read_traffic_per_S():
-    p = REPO / "profiles" / "ncu_search_batched.txt"
+def read_traffic_per_S(kernel: str):
+    """DRAM bytes per S of one kernel, from its committed ncu summary."""
+    p = REPO / "profiles" / f"ncu_{kernel}_5e9.txt"
     if not p.exists():
         return None
     m = re.search(r"^dram_bytes_per_S:\s*([\d.eE+-]+)", p.read_text(), re.M)
@@ -183,6 +322,12 @@ def main():
     ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of s4 work per reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--workload", choices=["exhaustive", "subranges", "triples", "serve"], default="exhaustive",
+                    help="exhaustive: the headline line (S < 1e10); the others print their own line")
+    ap.add_argument("--serve-requests", type=int, default=600)
+    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-triples", action="store_true")
     ap.add_argument("--range", type=int, nargs=2, default=None, metavar=("LO", "HI"),
                     help="search [LO, HI) instead of the rank's shard (a smaller case for ncu captures)")
     args = ap.parse_args()
@@ -191,6 +336,20 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank)
+    if args.workload != "exhaustive":
+        import torch
+        torch.cuda.set_device(local)
+        if rank != 0:
+            return
+        if args.workload == "subranges":
+            return run_subranges(args, local)
+        if args.workload == "serve":
+            return run_serve(args, local)
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        out = measure_triples(local, stream, steps=args.steps, warmup=args.warmup)
+        print(json.dumps({"metric": "triples_per_s", **out}), flush=True)
+        return
 
     import torch
     import torch.distributed as dist
@@ -258,6 +417,15 @@ def main():
     barrier()
     e2e_s = e0.elapsed_time(e1) / 1000.0
 
+    # per-kernel split of one step (events around every launch, direct launches)
+    with Search(hi, device=local, kernel=args.kernel, stream=stream.cuda_stream, time_kernels=True) as sk:
+        sk.enqueue(lo, hi)
+        sk.finish(want_lines=False)
+        flush.zero_()
+        sk.enqueue(lo, hi)
+        sk.finish(want_lines=False)
+        gen_ms, ext_ms = sk.last_kernel_split
+
     vals = torch.tensor([dev_s, e2e_s, kern_s], dtype=torch.float64, device="cuda")
     tot = torch.tensor([S_rank, cand_rank], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -291,6 +459,13 @@ def main():
                "sample": f"{len(slices)} slices of {slices[0][1] - slices[0][0]} S at the midpoints of 4 equal "
                          f"parts of [1,1e10), slowest region thread's own timer"}
 
+    triples = serving = None
+    if rank == 0 and world == 1 and args.range is None:
+        if not args.no_triples:
+            triples = measure_triples(local, stream)
+        if not args.no_serve:
+            serving = measure_serve(local, args.serve_requests, args.serve_rate)
+
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -298,8 +473,19 @@ def main():
         return
     sm_hz = (clk["sm_mhz"] or 1965.0) * 1e6
     peak = opmodel.issue_peak_lane_ops(props.multi_processor_count, sm_hz)
-    achieved = ops_launch / (kern_s / args.steps)
-    traffic_per_S = read_traffic_per_S()
+    achieved_step = ops_launch / (kern_s / args.steps)
+    ops_gen, ops_ext = opmodel.ops_split(stats)
+    kernels = {
+        "gen_jobs": {"ms_per_step": gen_ms, "ops_per_step": ops_gen,
+                     "achieved": ops_gen / (gen_ms / 1e3) if gen_ms else None,
+                     "traffic_per_step": (read_traffic_per_S("gen_jobs") or 0) * (hi - lo) or None},
+        "extend_jobs": {"ms_per_step": ext_ms, "ops_per_step": ops_ext,
+                        "achieved": ops_ext / (ext_ms / 1e3) if ext_ms else None,
+                        "traffic_per_step": (read_traffic_per_S("extend_jobs") or 0) * (hi - lo) or None},
+    }
+    for k in kernels.values():
+        k["frac"] = k["achieved"] / peak if k["achieved"] else None
+    dom = "extend_jobs" if ext_ms >= gen_ms else "gen_jobs"
     line = {
         "metric": METRIC, "value": S_all / dev_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
@@ -311,18 +497,23 @@ def main():
         "candidates_per_s": cand_all / dev_s,
         "sets4_per_s": stats["sets4"] * world * args.steps / dev_s,
         "kernel_ms_per_step": 1000 * kern_s / args.steps,
-        "roofline": {"bound": "int_issue", "achieved": achieved, "peak": peak, "unit": "lane-op/s",
-                     "frac": achieved / peak,
+        "roofline": {"bound": "int_issue", "kernel": dom, "achieved": kernels[dom]["achieved"], "peak": peak,
+                     "unit": "lane-op/s", "frac": kernels[dom]["frac"],
                      "peak_source": f"{props.multi_processor_count} SMs x 128 lanes x median SM clock under load "
                                     f"({sm_hz / 1e6:.0f} MHz sampled); MEASURED_PEAKS.json has no integer peak",
-                     "ops_per_launch": ops_launch,
-                     "traffic": traffic_per_S * (hi - lo) if traffic_per_S else None},
+                     "per": "step (all launches of the kernel in one search of the range; a step is "
+                            f"{launches // max(args.steps, 1) // 2} batches)",
+                     "ops": kernels[dom]["ops_per_step"], "traffic": kernels[dom]["traffic_per_step"],
+                     "step_achieved": achieved_step, "step_frac": achieved_step / peak,
+                     "kernels": kernels},
         "e2e": {"value": S_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
                 "d2h_bytes_per_step": d2h // args.steps, "result_lines": e2e_lines},
         "gpu_launches": launches,
         "clocks": clk,
         "plain_gpu": plain,
         "cpu_baseline": cpu,
+        "triples": triples,
+        "serving": serving,
     }
     print(json.dumps(line), flush=True)
 

@@ -64,7 +64,7 @@ typedef struct {
     uint32_t ctas_per_sm;  /* resident CTAs per SM for the persistent kernel; 0 = default            */
     void *stream;          /* cudaStream_t to launch on; NULL = a stream owned by the context        */
     uint32_t use_graph;    /* PS4_GRAPH_*: run a call's launch sequence as one captured CUDA graph   */
-    uint32_t reserved;
+    uint32_t time_kernels; /* 1: time every launch with events (ps4_last_kernel_split); no graphs     */
 } ps4_config;
 
 enum {
@@ -299,6 +299,9 @@ void ps4_graph_counts(const ps4_ctx *ctx, uint64_t *captures, uint64_t *replays)
 
 /* Device time (ms, CUDA events on the launch stream) of the kernels of the last search call. */
 double ps4_last_kernel_ms(const ps4_ctx *ctx);
+/* Device time (ms) of the last search call split by kernel: the tile kernel (4-set generation)
+ * and the extension engine, summed over the call's batches.  Needs time_kernels = 1. */
+void ps4_last_kernel_split(const ps4_ctx *ctx, double *gen_ms, double *ext_ms);
 /* Number of kernel launches made by the last search call. */
 uint64_t ps4_last_launches(const ps4_ctx *ctx);
 

@@ -65,6 +65,10 @@ struct ps4_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     std::string graph_key;
     uint64_t graph_launches = 0, graph_captures = 0, graph_replays = 0;
+    // per-launch timing (cfg.time_kernels): event pairs around each tile / engine launch
+    std::vector<cudaEvent_t> kev;
+    size_t kev_used = 0;
+    double gen_ms = 0.0, ext_ms = 0.0;
     // triple extension (grown on demand)
     uint64_t *d_tri_in = nullptr; uint64_t tri_in_cap = 0;
     uint8_t *d_tri_state = nullptr; uint64_t tri_state_cap = 0;
@@ -133,6 +137,7 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_segs) cudaFreeHost(c->h_segs);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
@@ -373,8 +378,18 @@ static int enqueue_items(ps4_ctx *c) {
 
     // A call of several batches runs as one CUDA graph holding its whole launch sequence; the
     // graph is kept and replayed while the next call is the same (items, sizes, buffers).
-    const bool graph = c->cfg.use_graph == PS4_GRAPH_ALWAYS ||
-                       (c->cfg.use_graph == PS4_GRAPH_AUTO && kernel == PS4_KERNEL_BATCHED && batch_start.size() >= 2);
+    const bool graph = !c->cfg.time_kernels &&
+                       (c->cfg.use_graph == PS4_GRAPH_ALWAYS ||
+                        (c->cfg.use_graph == PS4_GRAPH_AUTO && kernel == PS4_KERNEL_BATCHED && batch_start.size() >= 2));
+    const bool timed = c->cfg.time_kernels && kernel == PS4_KERNEL_BATCHED;
+    c->kev_used = 0;
+    if (timed) {                                  // 4 events per batch: gen start/end, ext start/end
+        while (c->kev.size() < 4 * batch_start.size()) {
+            cudaEvent_t e;
+            CUDA_TRY(c, cudaEventCreate(&e));
+            c->kev.push_back(e);
+        }
+    }
     std::string key;
     if (graph) {
         key.append(reinterpret_cast<const char *>(segs.data()), segs.size() * sizeof(Item));
@@ -410,12 +425,17 @@ static int enqueue_items(ps4_ctx *c) {
                 const int g = (int)std::min<uint64_t>((uint64_t)g_gen, std::max<uint64_t>(a.n_tiles, 1));
                 // n_jobs, tile_next, ext_next: the per-batch tail of the status block
                 e = cudaMemsetAsync(&c->d_status->n_jobs, 0, 2 * sizeof(unsigned long long), c->stream);
+                if (timed && e == cudaSuccess) e = cudaEventRecord(c->kev[4 * b], c->stream);
                 if (e == cudaSuccess) e = (cudaError_t)launch_gen(a, g, c->stream);
+                if (timed && e == cudaSuccess) e = cudaEventRecord(c->kev[4 * b + 1], c->stream);
                 c->last_launches++;
                 if (e == cudaSuccess && ext) {
-                    e = (cudaError_t)launch_ext(a, g_ext, c->stream);
+                    if (timed) e = cudaEventRecord(c->kev[4 * b + 2], c->stream);
+                    if (e == cudaSuccess) e = (cudaError_t)launch_ext(a, g_ext, c->stream);
+                    if (timed && e == cudaSuccess) e = cudaEventRecord(c->kev[4 * b + 3], c->stream);
                     c->last_launches++;
                 }
+                if (timed) c->kev_used = 4 * (b + 1);
             }
         } else if (e == cudaSuccess && tiles_total > 0) {
             a.items = c->d_items; a.n_items = (uint32_t)segs.size(); a.n_tiles = tiles_total;
@@ -431,6 +451,7 @@ static int enqueue_items(ps4_ctx *c) {
             if (e == cudaSuccess) e = e2;
             if (e == cudaSuccess) {
                 if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
                 c->graph_exec = nullptr;
                 c->graph_key.clear();
                 e = cudaGraphInstantiate(&c->graph_exec, g, 0);
@@ -507,6 +528,15 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, c->ev0, c->ev1);
             c->last_ms = ms;                     // the attempt whose results are kept
+            c->gen_ms = c->ext_ms = 0.0;
+            const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
+            for (size_t i = 0; i + 3 < c->kev_used; i += 4) {
+                float g = 0.f, x = 0.f;
+                cudaEventElapsedTime(&g, c->kev[i], c->kev[i + 1]);
+                if (ext) cudaEventElapsedTime(&x, c->kev[i + 2], c->kev[i + 3]);
+                c->gen_ms += g;
+                c->ext_ms += x;
+            }
         }
         const Status &st = *c->h_status;
         const unsigned code = (unsigned)(st.err & 0xFF);
@@ -663,6 +693,11 @@ extern "C" void ps4_get_tuning(const ps4_ctx *c, ps4_tuning *t) {
     while ((1ull << lj) < c->jobs_cap_max) lj++;
     t->log2_jobs = lj;
     t->rate = c->tuned_rate;
+}
+
+extern "C" void ps4_last_kernel_split(const ps4_ctx *c, double *gen_ms, double *ext_ms) {
+    if (gen_ms) *gen_ms = c ? c->gen_ms : 0.0;
+    if (ext_ms) *ext_ms = c ? c->ext_ms : 0.0;
 }
 
 extern "C" void ps4_graph_counts(const ps4_ctx *c, uint64_t *captures, uint64_t *replays) {

@@ -49,7 +49,7 @@ class Config(C.Structure):
     _fields_ = [("device", C.c_int), ("s_hi_max", C.c_uint64), ("cap_reps", C.c_uint32),
                 ("cap_divs", C.c_uint32), ("cap_ext", C.c_uint32), ("flags", C.c_uint32),
                 ("kernel", C.c_uint32), ("log2_tile", C.c_uint32), ("ctas_per_sm", C.c_uint32),
-                ("stream", C.c_void_p), ("use_graph", C.c_uint32), ("reserved", C.c_uint32)]
+                ("stream", C.c_void_p), ("use_graph", C.c_uint32), ("time_kernels", C.c_uint32)]
 
 
 class Tuning(C.Structure):
@@ -144,6 +144,7 @@ def load() -> C.CDLL:
         "ps4_set_tuning": (C.c_int, [C.c_void_p, P(Tuning)]),
         "ps4_get_tuning": (None, [C.c_void_p, P(Tuning)]),
         "ps4_graph_counts": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
+        "ps4_last_kernel_split": (None, [C.c_void_p, P(C.c_double), P(C.c_double)]),
         "ps4_format_hit": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),
         "ps4_format_six": (C.c_long, [P(Hit), P(Ext), P(Six), C.c_char_p, C.c_size_t]),
         "ps4_format_drill": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),

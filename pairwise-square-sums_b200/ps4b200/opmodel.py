@@ -20,6 +20,20 @@ def ops(stats: dict) -> int:
     return sum(w * int(stats[k]) for k, w in WEIGHTS.items())
 
 
+# Which kernel of the two-kernel pipeline does which part of the work: the tile kernel
+# (gen_jobs) enumerates representations and combines them; the extension engine
+# (extend_jobs) sets up each 4-set (divisor counts, factor walks, residues) and walks and
+# tests its divisor pairs.
+GEN_EVENTS = ("pairs", "triples")
+EXT_EVENTS = ("sets4", "ext_cand", "ext_sqrt")
+
+
+def ops_split(stats: dict) -> tuple[int, int]:
+    """(tile-kernel ops, engine ops) of the model above."""
+    return (sum(WEIGHTS[k] * int(stats[k]) for k in GEN_EVENTS),
+            sum(WEIGHTS[k] * int(stats[k]) for k in EXT_EVENTS))
+
+
 def issue_peak_lane_ops(num_sms: int, sm_clock_hz: float) -> float:
     """Integer issue ceiling: 4 schedulers x 32 lanes per SM per clock."""
     return num_sms * 4 * 32 * sm_clock_hz

@@ -44,7 +44,7 @@ class Search:
     def __init__(self, s_hi_max: int, device: int = 0, *, noext: bool = False, verify: bool = False,
                  dump4: bool = False, kernel: str = "batched", cap_reps: int = 0, cap_divs: int = 0,
                  cap_ext: int = 0, log2_tile: int = 0, ctas_per_sm: int = 0, stream: int | None = None,
-                 graph: str = "auto"):
+                 graph: str = "auto", time_kernels: bool = False):
         self.lib = _abi.load()
         cfg = _abi.Config()
         cfg.device = device
@@ -59,6 +59,7 @@ class Search:
         cfg.stream = stream
         cfg.use_graph = {"auto": _abi.PS4_GRAPH_AUTO, "always": _abi.PS4_GRAPH_ALWAYS,
                          "never": _abi.PS4_GRAPH_NEVER}[graph]
+        cfg.time_kernels = 1 if time_kernels else 0
         self.dump4 = dump4
         self.ctx = C.c_void_p()
         rc = self.lib.ps4_create(C.byref(cfg), C.byref(self.ctx))
@@ -184,6 +185,13 @@ class Search:
         t = _abi.Tuning(d["log2_tile"], d["gen_ctas"], d["ext_ctas"], d["log2_jobs"], d.get("rate", 0.0))
         self._call(lambda: self.lib.ps4_set_tuning(self.ctx, C.byref(t)))
 
+    @property
+    def last_kernel_split(self) -> tuple[float, float]:
+        """(tile kernel ms, extension engine ms) of the last call (needs time_kernels=True)."""
+        g, x = C.c_double(), C.c_double()
+        self.lib.ps4_last_kernel_split(self.ctx, C.byref(g), C.byref(x))
+        return float(g.value), float(x.value)
+
     def graph_counts(self) -> tuple[int, int]:
         """(CUDA graphs captured, graph replays) on this context so far."""
         a, b = C.c_uint64(), C.c_uint64()
@@ -208,20 +216,25 @@ class Search:
             self._collect(out)
         return [s.as_dict() for s in st], out
 
-    def extend_triples(self, abc, dmax: int):
+    def extend_triples(self, abc, dmax: int, *, as_lists: bool = True):
         """Every d <= dmax extending each square-sum triple (rows of ``abc``) to a 4-set.
 
         Returns (exts, state, stats): exts[i] the sorted extensions of triple i, state[i] 0 for
         a searched triple and 1 for a row that is not a square-sum triple of distinct positive
-        integers, stats the call's counters."""
+        integers, stats the call's counters.  With as_lists=False exts is the record array
+        (fields d, item) sorted by (item, d) instead of per-triple lists."""
         import numpy as np
-        a = np.ascontiguousarray(np.asarray(abc, dtype=np.uint64).reshape(-1, 3))
+        a = abc if (isinstance(abc, np.ndarray) and abc.dtype == np.uint64 and abc.flags.c_contiguous
+                    and abc.ndim == 2) else np.ascontiguousarray(np.asarray(abc, dtype=np.uint64).reshape(-1, 3))
         n = a.shape[0]
         state = np.zeros(max(n, 1), dtype=np.uint8)
         cap = max(self._tri_cap, 1024) if hasattr(self, "_tri_cap") else 1 << 16
         st = _abi.TriStats()
         while True:
-            out = (_abi.TriExt * cap)()
+            out = self._tri_buf if getattr(self, "_tri_buf", None) is not None and len(self._tri_buf) >= cap \
+                else (_abi.TriExt * cap)()
+            self._tri_buf = out
+            cap = len(out)
             n_out = C.c_uint64()
             rc = self.lib.ps4_extend_triples(self.ctx, a.ctypes.data, n, int(dmax), state.ctypes.data, out, cap,
                                              C.byref(n_out), C.byref(st))
@@ -234,6 +247,8 @@ class Search:
         self._tri_cap = cap
         recs = np.frombuffer(out, dtype=np.dtype([("d", "<u8"), ("item", "<u4"), ("reserved", "<u4")]),
                              count=int(n_out.value))
+        if not as_lists:
+            return recs.copy(), state[:n], st.as_dict()
         exts = [[] for _ in range(n)]
         for d, item in zip(recs["d"].tolist(), recs["item"].tolist()):
             exts[item].append(d)
