@@ -365,21 +365,35 @@ __device__ __forceinline__ void tile_bounds(const SearchArgs &a, uint64_t tile, 
     n = (uint32_t)(S1 - S0);
 }
 
+// floor(sqrt(x)) for x < 2^46: a float estimate is within one unit of the root (the root is
+// < 2^23 and float carries 24 bits), then exact integer correction (products < 2^47).
+__device__ __forceinline__ uint32_t isqrt_lt2p46(uint64_t x) {
+    uint32_t r = (uint32_t)sqrtf((float)x);
+    while ((uint64_t)r * r > x) r--;
+    while ((uint64_t)(r + 1) * (r + 1) <= x) r++;
+    return r;
+}
+
 // P1 / P3: scan every representation S = p^2 + q^2, 1 <= p <= q, S in [S0, S0+n).
-// q-major: q runs over [ceil(sqrt(S0/2)), isqrt(S1-2)], p from ceil(sqrt(S0-q^2)).
+// q-major: q runs over [ceil(sqrt(S0/2)), isqrt(S1-2)] (strided over the threads), p from
+// ceil(sqrt(S0-q^2)) by a float estimate with exact integer correction (S < 2^44).
 template <bool FILL>
 __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t *cnt32, uint32_t *rep_p,
                                               uint32_t *rep_q) {
     const uint64_t S1 = S0 + n;
-    uint64_t qmin = ceil_sqrt64((S0 + 1) >> 1);
+    uint32_t qmin = (uint32_t)ceil_sqrt64((S0 + 1) >> 1);
     if (qmin < 1) qmin = 1;
-    const uint64_t qmax = S1 >= 2 ? isqrt64(S1 - 2) : 0;
+    const uint32_t qmax = S1 >= 2 ? (uint32_t)isqrt64(S1 - 2) : 0;
     uint32_t found = 0;
-    for (uint64_t q = qmin + threadIdx.x; q <= qmax; q += BS) {
-        const uint64_t q2 = q * q;
-        uint64_t p = 1;
-        if (S0 > q2 + 1) p = ceil_sqrt64(S0 - q2);
-        for (uint64_t s = p * p + q2; p <= q && s < S1; s += 2 * p + 1, p++) {
+    for (uint32_t q = qmin + threadIdx.x; q <= qmax; q += BS) {
+        const uint64_t q2 = (uint64_t)q * q;
+        uint32_t p = 1;
+        if (S0 > q2 + 1) {
+            const uint64_t m = S0 - q2;                // p = ceil(sqrt(m))
+            const uint32_t r = isqrt_lt2p46(m);
+            p = r + ((uint64_t)r * r < m ? 1u : 0u);
+        }
+        for (uint64_t s = (uint64_t)p * p + q2; p <= q && s < S1; s += 2 * p + 1, p++) {
             const uint32_t i = (uint32_t)(s - S0), w = i >> 1, sh = (i & 1) * 16;
             if (!FILL) {
                 atomicAdd(&cnt32[w], 1u << sh);
@@ -388,8 +402,8 @@ __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t 
                 const uint32_t cur = (((volatile uint32_t *)cnt32)[w] >> sh) & 0xFFFFu;
                 if (cur == 0xFFFFu) continue;          // S not selected
                 const uint32_t pos = (atomicAdd(&cnt32[w], 1u << sh) >> sh) & 0xFFFFu;
-                rep_p[pos] = (uint32_t)p;
-                rep_q[pos] = (uint32_t)q;
+                rep_p[pos] = p;
+                rep_q[pos] = q;
             }
         }
     }

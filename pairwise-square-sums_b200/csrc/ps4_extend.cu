@@ -216,15 +216,6 @@ __device__ __forceinline__ void rot65(uint32_t a, uint64_t &lo, uint32_t &bit64)
     bit64 = (uint32_t)(Y >> 64) & 1u;
 }
 
-// floor(sqrt(x)) for x < 2^46: a float estimate is within one unit of the root (the root is
-// < 2^23, and float carries 24 bits), then exact integer correction.
-__device__ __forceinline__ uint32_t isqrt_lt2p46(uint64_t x) {
-    uint32_t r = (uint32_t)sqrtf((float)x);
-    while ((uint64_t)r * r > x) r--;
-    while ((uint64_t)(r + 1) * (r + 1) <= x) r++;
-    return r;
-}
-
 // (d mod 63, d mod 65) for |d| < 2^48, by folding 24-bit halves (2^24 = 1 mod 63 and mod 65)
 __device__ __forceinline__ void res6365(int64_t d, uint32_t &r63, uint32_t &r65) {
     const uint64_t x = d < 0 ? (uint64_t)(-d) : (uint64_t)d;

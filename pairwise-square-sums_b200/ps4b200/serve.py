@@ -156,6 +156,7 @@ class Server:
 @dataclass
 class StreamReport:
     latency_s: dict = field(default_factory=dict)     # rid -> seconds from arrival to finish
+    done: dict = field(default_factory=dict)          # rid -> the finish record (steps, reruns, times)
     results: dict = field(default_factory=dict)       # rid -> RangeResult / (exts, state, stats) / Ps4Error
     wall_s: float = 0.0
     info: dict = field(default_factory=dict)
@@ -189,6 +190,7 @@ def run_stream(server: Server, reqs, *, collect: bool = True, max_wait_us: int =
         for d in server.progress(wait):
             r = by_tag[d["tag"]]
             rep.latency_s[r.rid] = d["t_done"] - (t0 + r.t_arrive)
+            rep.done[r.rid] = d
             finished += 1
             if d["status"] != _abi.PS4_OK:
                 try:

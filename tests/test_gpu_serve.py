@@ -39,8 +39,9 @@ def test_mixed_stream_matches_alone(search):
     assert len(rep.results) == len(rep.latency_s) == len(reqs)
     for r in reqs:
         _check_same(search, r, rep.results[r.rid])
-    # queries share steps: far fewer steps than queries
-    assert 2 <= rep.info["steps"] < len(reqs) // 2
+    # queries share steps: the steps that carried each query add up to more than the steps run
+    assert rep.info["steps"] >= 2
+    assert sum(d["steps"] for d in rep.done.values()) > rep.info["steps"]
     assert rep.info["waiting"] == rep.info["active"] == 0 and rep.info["arena_used"] == 0
     assert rep.percentile(50) > 0
 
