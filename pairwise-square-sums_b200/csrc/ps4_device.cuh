@@ -137,24 +137,32 @@ __device__ __forceinline__ void choose_pair(const uint64_t v[4], const uint32_t 
     }
 }
 
+// Factor table entry of m >= 2 (build_tables): its smallest prime p (bits 0..23), the exponent
+// of p in m (bits 24..31) and the cofactor m / p^e (bits 32..63), so a walk takes one
+// dependent load per distinct prime.
+__device__ __forceinline__ uint32_t spf_p(uint64_t t) { return (uint32_t)t & 0xFFFFFFu; }
+__device__ __forceinline__ uint32_t spf_e(uint64_t t) { return ((uint32_t)t >> 24) & 0xFFu; }
+__device__ __forceinline__ uint32_t spf_cof(uint64_t t) { return (uint32_t)(t >> 32); }
+
 // Merge the factorisation of m into (pr, ex, np), primes in first-seen order of the
-// smallest-prime-factor walk (s4.c:141-147).
+// smallest-prime-factor walk (s4.c:141-147): ascending within m.  The power of two is
+// taken by counting trailing zeros.
 __device__ __forceinline__ void factor_merge(const uint64_t *spfq, uint32_t m, uint32_t *pr, uint8_t *ex, int &np) {
-    while (m > 1) {
-        uint64_t sq = __ldg(&spfq[m]);
-        const uint32_t p = (uint32_t)sq;
-        int e = 0;
-        for (;;) {
-            m = (uint32_t)(sq >> 32);
-            e++;
-            if (m <= 1) break;
-            sq = __ldg(&spfq[m]);
-            if ((uint32_t)sq != p) break;
-        }
+    auto merge = [&](uint32_t p, uint32_t e) {
         int i = 0;
         while (i < np && pr[i] != p) i++;
         if (i == np) { pr[np] = p; ex[np] = 0; np++; }
         ex[i] = (uint8_t)(ex[i] + e);
+    };
+    if (m > 1 && !(m & 1)) {
+        const uint32_t z = (uint32_t)__ffs((int)m) - 1;
+        merge(2, z);
+        m >>= z;
+    }
+    while (m > 1) {
+        const uint64_t t = __ldg(&spfq[m]);
+        merge(spf_p(t), spf_e(t));
+        m = spf_cof(t);
     }
 }
 

@@ -342,41 +342,40 @@ struct LaneJob {
     uint32_t ndo, nd, ncand, L, H;
 };
 
-// Returns false if the 4-set's difference has more divisors than cap_divs (fatal).
-// Factor D = m1*m2 (m1 = ra-rb, m2 = ra+rb, both < 2^23, so at most 7 distinct primes each):
-// the two smallest-prime-factor walks run interleaved so that their dependent table loads
-// overlap; m1's primes are stored from slot 0, m2's from slot 8, then m2's are merged into
-// m1's list -- primes in first-seen order, as s4.c:141-147.  A new prime is written to a slot
-// below every unread slot of m2, so the merge is in place.
+// Factor D = m1*m2 (m1 = ra-rb, m2 = ra+rb, both < 2^23, of equal parity).  The power of two
+// comes from counting trailing zeros; the odd parts' walks (one table load per distinct prime)
+// run interleaved so that their dependent loads overlap.  m1's primes are stored from slot 0,
+// m2's from slot 8 (each has at most 7 distinct odd primes), then m2's are merged into m1's
+// list -- primes in first-seen order, as s4.c:141-147.  A new prime is written to a slot below
+// every unread slot of m2, so the merge is in place.
 __device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, uint32_t m2, uint32_t (*fp)[32],
                                            uint8_t (*fe)[32], int lane) {
     int na = 0, nb = 0;
-    uint32_t pa = 0, pb = 0, ea = 0, eb = 0;
+    if (m1 > 1 && !(m1 & 1)) {                      // both even
+        const uint32_t z1 = (uint32_t)__ffs((int)m1) - 1, z2 = (uint32_t)__ffs((int)m2) - 1;
+        fp[0][lane] = 2;
+        fe[0][lane] = (uint8_t)(z1 + z2);
+        na = 1;
+        m1 >>= z1;
+        m2 >>= z2;
+    }
     uint64_t sa = m1 > 1 ? __ldg(&spfq[m1]) : 0, sb = m2 > 1 ? __ldg(&spfq[m2]) : 0;
     while (m1 > 1 || m2 > 1) {
         if (m1 > 1) {
-            const uint32_t p = (uint32_t)sa;
-            if (p != pa) {
-                if (ea) { fp[na][lane] = pa; fe[na][lane] = (uint8_t)ea; na++; }
-                pa = p; ea = 0;
-            }
-            ea++;
-            m1 = (uint32_t)(sa >> 32);
+            fp[na][lane] = spf_p(sa);
+            fe[na][lane] = (uint8_t)spf_e(sa);
+            na++;
+            m1 = spf_cof(sa);
             if (m1 > 1) sa = __ldg(&spfq[m1]);
         }
         if (m2 > 1) {
-            const uint32_t p = (uint32_t)sb;
-            if (p != pb) {
-                if (eb) { fp[8 + nb][lane] = pb; fe[8 + nb][lane] = (uint8_t)eb; nb++; }
-                pb = p; eb = 0;
-            }
-            eb++;
-            m2 = (uint32_t)(sb >> 32);
+            fp[8 + nb][lane] = spf_p(sb);
+            fe[8 + nb][lane] = (uint8_t)spf_e(sb);
+            nb++;
+            m2 = spf_cof(sb);
             if (m2 > 1) sb = __ldg(&spfq[m2]);
         }
     }
-    if (ea) { fp[na][lane] = pa; fe[na][lane] = (uint8_t)ea; na++; }
-    if (eb) { fp[8 + nb][lane] = pb; fe[8 + nb][lane] = (uint8_t)eb; nb++; }
     int np = na;
     for (int j = 0; j < nb; j++) {
         const uint32_t p = fp[8 + j][lane];

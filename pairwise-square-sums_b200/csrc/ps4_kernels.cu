@@ -273,20 +273,23 @@ __global__ void __launch_bounds__(BS, 1) search_plain(const SearchArgs a) {
 __global__ void build_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t n) {
     for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n; m += (uint64_t)gridDim.x * blockDim.x) {
         if (m < 2) {
-            spfq[m] = m | (m << 32);
+            spfq[m] = 0;
             ndiv[m] = (uint16_t)m;
             continue;
         }
-        uint32_t x = (uint32_t)m, sp = 0, nd = 1;
+        // entry: smallest prime p | its exponent e << 24 | cofactor m / p^e << 32
+        uint32_t x = (uint32_t)m, sp = 0, se = 0, nd = 1;
         for (uint32_t d = 2; d * d <= x; d += (d == 2 ? 1 : 2)) {
             if (x % d) continue;
-            if (!sp) sp = d;
             uint32_t e = 0;
             while (x % d == 0) { x /= d; e++; }
+            if (!sp) { sp = d; se = e; }
             nd *= e + 1;
         }
-        if (x > 1) { if (!sp) sp = x; nd *= 2; }
-        spfq[m] = (uint64_t)sp | ((uint64_t)((uint32_t)m / sp) << 32);
+        if (x > 1) { if (!sp) { sp = x; se = 1; } nd *= 2; }
+        uint32_t cof = (uint32_t)m;
+        for (uint32_t e = 0; e < se; e++) cof /= sp;
+        spfq[m] = (uint64_t)sp | ((uint64_t)se << 24) | ((uint64_t)cof << 32);
         ndiv[m] = (uint16_t)nd;
     }
 }
