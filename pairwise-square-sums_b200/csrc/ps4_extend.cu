@@ -201,20 +201,38 @@ struct WarpArea {
 
 static_assert(EWARPS * sizeof(WarpArea) + 1024 <= 228 * 1024 / 3, "three engine CTAs per SM");
 
-// Rotated residue masks: bit s of the result is QR_m[(s + a) mod m], so the test of
-// e + C = u^2 + (C - A) becomes one shift of the mask by u^2 mod m.
-__device__ __forceinline__ uint64_t rot64(uint64_t x, uint32_t a) { return a ? (x >> a) | (x << (64 - a)) : x; }
-__device__ __forceinline__ uint64_t rot63(uint64_t x, uint32_t a) {
-    const uint64_t M = (1ull << 63) - 1;
-    return a ? ((x >> a) | (x << (63 - a))) & M : x;
+// Residue masks indexed by u's residue: bit w of q_m[a] is set iff w^2 + a is a square mod m.
+// A 4-set's mask for its two remaining members C1, C2 is q_m[(C1-A) mod m] & q_m[(C2-A) mod m],
+// so the filters of e + C = u^2 + (C - A) (s4.c:192-194) become one bit test per modulus on
+// u mod m.  Mod 65 needs 65 bits: bit 64 lives in q65top.
+struct UResTabs {
+    uint64_t q64[64], q63[63], q65[65];
+    uint8_t q65top[65];
+};
+constexpr bool is_qr_mod(int m, int r) {
+    return r < 64 ? ((qr_bits(m) >> r) & 1) != 0 : true;          // r = 64 (m = 65) is 8^2
 }
-__device__ __forceinline__ void rot65(uint32_t a, uint64_t &lo, uint32_t &bit64) {
-    const u128 X = (u128)QR65 | ((u128)1 << 64);            // residue 64 = 8^2 is a square
-    const u128 M = ((u128)1 << 65) - 1;
-    const u128 Y = a ? ((X >> a) | (X << (65 - a))) & M : X;
-    lo = (uint64_t)Y;
-    bit64 = (uint32_t)(Y >> 64) & 1u;
+constexpr UResTabs make_ures() {
+    UResTabs t{};
+    for (int a = 0; a < 64; a++) {
+        uint64_t x = 0;
+        for (int w = 0; w < 64; w++) if (is_qr_mod(64, (w * w + a) % 64)) x |= 1ull << w;
+        t.q64[a] = x;
+    }
+    for (int a = 0; a < 63; a++) {
+        uint64_t x = 0;
+        for (int w = 0; w < 63; w++) if (is_qr_mod(63, (w * w + a) % 63)) x |= 1ull << w;
+        t.q63[a] = x;
+    }
+    for (int a = 0; a < 65; a++) {
+        uint64_t x = 0;
+        for (int w = 0; w < 64; w++) if (is_qr_mod(65, (w * w + a) % 65)) x |= 1ull << w;
+        t.q65[a] = x;
+        t.q65top[a] = is_qr_mod(65, (64 * 64 + a) % 65) ? 1 : 0;
+    }
+    return t;
 }
+__device__ const UResTabs UQ = make_ures();
 
 // (d mod 63, d mod 65) for |d| < 2^48, by folding 24-bit halves (2^24 = 1 mod 63 and mod 65)
 __device__ __forceinline__ void res6365(int64_t d, uint32_t &r63, uint32_t &r65) {
@@ -533,15 +551,13 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 EJob &E = w->job[lane];
                 E.A = J.A; E.C1 = J.C1; E.C2 = J.C2;
                 const int64_t dd1 = (int64_t)J.C1 - (int64_t)J.A, dd2 = (int64_t)J.C2 - (int64_t)J.A;
-                uint32_t a63, a65, b63, b65, h1, h2;
+                uint32_t a63, a65, b63, b65;
                 res6365(dd1, a63, a65);
                 res6365(dd2, b63, b65);
-                E.m64 = rot64(QR64, (uint32_t)dd1 & 63u) & rot64(QR64, (uint32_t)dd2 & 63u);
-                E.m63 = rot63(QR63, a63) & rot63(QR63, b63);
-                uint64_t m65a, m65b;
-                rot65(a65, m65a, h1);
-                rot65(b65, m65b, h2);
-                E.m65 = m65a & m65b;
+                E.m64 = UQ.q64[(uint32_t)dd1 & 63u] & UQ.q64[(uint32_t)dd2 & 63u];
+                E.m63 = UQ.q63[a63] & UQ.q63[b63];
+                E.m65 = UQ.q65[a65] & UQ.q65[b65];
+                const uint32_t h1 = UQ.q65top[a65], h2 = UQ.q65top[b65];
                 uint64_t vmax = J.v[0];
                 for (int i = 1; i < 4; i++) vmax = J.v[i] > vmax ? J.v[i] : vmax;
                 E.uA = isqrt_lt2p46(J.A);                        // < 2^22 (A < 2^44)
@@ -613,13 +629,13 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     // f = 2^d2 * lo[l]*hi[h], g = 2^(E2-d2) * lo[L-1-l]*hi[H-1-h]: complementary divisors
                     const uint64_t fo = w->dbuf[jb + l] * hv, go = w->dbuf[jb + L - 1 - l] * hc;
                     u = ((fo << d2) + (go << (E2 - d2))) >> 1;
-                    // e + C = u^2 + (C - A): residues mod 64, 63, 65 for both C (s4.c:192-194)
+                    // e + C = u^2 + (C - A): residues mod 64, 63, 65 for both C (s4.c:192-194), as
+                    // bits of the 4-set's u-indexed masks
                     const uint32_t w64 = (uint32_t)u & 63u;
                     const uint32_t rr = (uint32_t)(u >> 24) + ((uint32_t)u & 0xFFFFFFu);   // 2^24 = 1 mod 63, 65
                     const uint32_t w63 = rr % 63u, w65 = rr % 65u;
-                    const uint32_t s64 = (w64 * w64) & 63u, s63 = (w63 * w63) % 63u, s65 = (w65 * w65) % 65u;
-                    const uint32_t b65 = s65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65 >> s65) & 1u;
-                    pass = (((m64 >> s64) & (m63 >> s63) & 1u) & b65) && u > uA;
+                    const uint32_t b65 = w65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65 >> w65) & 1u;
+                    pass = (((m64 >> w64) & (m63 >> w63) & 1u) & b65) && u > uA;
                     if (pass && u <= uS) {                  // e <= max(v): rule out e in v (s4.c:197)
                         const uint64_t e = u * u - A;       // u < 2^23
                         const EJob &Ej = w->job[jcur];
