@@ -594,7 +594,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             // the current job of this lane's run, in registers
             uint64_t A = 0, m64 = 0, m63 = 0, m65 = 0, hv = 0, hc = 0;
             uint32_t uA = 0, uS = 0;
-            uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1;
+            uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1, dlo = 0, dhi = 0;
             uint32_t cc = 0, l = 0, h = 0, d2 = 0;
             // job fields in four vector loads; entering a job at its first candidate needs no division
             auto load_job = [&](uint32_t j) {
@@ -606,6 +606,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 uA = y.x; uS = y.y; ncand = y.z;
                 jb = z.x & 0xFFFFu; L = z.x >> 16; H = z.y & 0xFFFFu; E2 = (z.y >> 16) & 0xFFu; flg = z.y >> 24;
                 R = (flg & 1) ? E2 - 1 : 1;
+                dlo = flg & 1; dhi = (flg & 1) ? E2 - 1 : 0;      // 2-exponents of f: [1, E2-1] or {0}
                 cnt.use(a, y.w);
                 cc = 0; l = 0; h = 0; d2 = (flg & 1) ? 1u : 0u;
             };
@@ -643,9 +644,15 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     }
                     if (pass) { cnt.sqrt_++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
-                    if (flg & 1) {
-                        if (++d2 > R) { d2 = 1; if (++l == L) { l = 0; h++; } }
-                    } else if (++l == L) { l = 0; h++; }
+                    {                                          // (l, h, d2) advance, branch-free
+                        d2++;
+                        const uint32_t wd = d2 > dhi ? 1u : 0u;
+                        d2 = wd ? dlo : d2;
+                        l += wd;
+                        const uint32_t wl = l == L ? 1u : 0u;
+                        l = wl ? 0u : l;
+                        h += wl;
+                    }
                     if (++cc == ncand && it + 1 < g1 - g0) {
                         do { jl++; } while (jl < 31 && w->cstart[jl + 1] == w->cstart[jl]);
                         load_job(jl);
