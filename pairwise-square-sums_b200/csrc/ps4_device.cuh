@@ -335,6 +335,7 @@ struct TileShared {
     uint32_t elist_n, work;
     uint32_t binhist[NBIN], binstart[NBIN];
     uint32_t skip;             // tile abandoned (error)
+    uint32_t raw_n[NWARP];     // representations each warp appended to the tile's raw list
     uint64_t tile;
 };
 
@@ -387,7 +388,8 @@ __device__ __forceinline__ uint32_t isqrt_lt2p46(uint64_t x) {
 // ceil(sqrt(S0-q^2)) by a float estimate with exact integer correction (S < 2^44).
 template <bool FILL>
 __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t *cnt32, uint32_t *rep_p,
-                                              uint32_t *rep_q) {
+                                              uint32_t *rep_q, uint64_t *raw = nullptr, uint32_t *raw_n = nullptr,
+                                              uint32_t slice = 0) {
     const uint64_t S1 = S0 + n;
     uint32_t qmin = (uint32_t)ceil_sqrt64((S0 + 1) >> 1);
     if (qmin < 1) qmin = 1;
@@ -406,6 +408,15 @@ __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t 
             if (!FILL) {
                 atomicAdd(&cnt32[w], 1u << sh);
                 found++;
+                if (raw) {                                 // warp-aggregated append to this warp's slice
+                    const unsigned am = __activemask();
+                    const int lane = threadIdx.x & 31, lead = __ffs(am) - 1;
+                    uint32_t base = 0;
+                    if (lane == lead) base = atomicAdd(raw_n, (uint32_t)__popc(am));
+                    base = __shfl_sync(am, base, lead);
+                    const uint32_t pos = base + __popc(am & ((1u << lane) - 1u));
+                    if (pos < slice) raw[pos] = (uint64_t)i | ((uint64_t)p << 14) | ((uint64_t)q << 36);
+                }
             } else {
                 const uint32_t cur = (((volatile uint32_t *)cnt32)[w] >> sh) & 0xFFFFu;
                 if (cur == 0xFFFFu) continue;          // S not selected
@@ -433,8 +444,12 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
 
     for (uint32_t i = tid; i < L::W / 2; i += BS) cnt32[i] = 0;
     __syncthreads();
-    // P1: count
-    const uint32_t found = scan_reps<false>(S0, n, cnt32, rep_p, rep_q);
+    // P1: count -- and, given a raw list and a tile from RAW_MIN_S up, record every representation
+    // (p <= q < 2^22, offset < 2^14) so that P3 need not scan again
+    const bool use_raw = a.raw != nullptr && S0 >= RAW_MIN_S;
+    const uint32_t slice = use_raw ? a.raw_cap / NWARP : 0;
+    uint64_t *raw_w = use_raw ? a.raw + (size_t)blockIdx.x * a.raw_cap + (size_t)(tid >> 5) * slice : nullptr;
+    const uint32_t found = scan_reps<false>(S0, n, cnt32, rep_p, rep_q, raw_w, &ts.raw_n[tid >> 5], slice);
     ull f = warp_sum((ull)found);
     if ((tid & 31) == 0 && f) atomicAdd(&ts.cnt[K_PAIRS], f);
     __syncthreads();
@@ -498,8 +513,26 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
         cnt32[i >> 1] = word;
     }
     __syncthreads();
-    // P3: fill
-    scan_reps<true>(S0, n, cnt32, rep_p, rep_q);
+    // P3: fill, from the raw list when every warp's slice held its representations
+    bool from_raw = use_raw;
+    for (int w = 0; w < NWARP; w++) from_raw = from_raw && ts.raw_n[w] <= slice;
+    if (from_raw) {
+        const uint64_t *raw = a.raw + (size_t)blockIdx.x * a.raw_cap;
+        for (int w = 0; w < NWARP; w++) {
+            const uint32_t cw = ts.raw_n[w];
+            for (uint32_t o = tid; o < cw; o += BS) {
+                const uint64_t e = raw[(size_t)w * slice + o];
+                const uint32_t i = (uint32_t)e & 0x3FFFu, wd = i >> 1, sh = (i & 1) * 16;
+                const uint32_t cur = (((volatile uint32_t *)cnt32)[wd] >> sh) & 0xFFFFu;
+                if (cur == 0xFFFFu) continue;          // S not selected
+                const uint32_t pos = (atomicAdd(&cnt32[wd], 1u << sh) >> sh) & 0xFFFFu;
+                rep_p[pos] = (uint32_t)(e >> 14) & 0x3FFFFFu;
+                rep_q[pos] = (uint32_t)(e >> 36);
+            }
+        }
+    } else {
+        scan_reps<true>(S0, n, cnt32, rep_p, rep_q);
+    }
     __syncthreads();
     // P4: each list ascending in p
     for (uint32_t s = tid; s < ts.n_is; s += BS) {
@@ -644,6 +677,7 @@ __device__ __forceinline__ void tile_flush_counters(const SearchArgs &a, TileSha
 __device__ __forceinline__ void tile_reset(TileShared &ts) {
     if (threadIdx.x < 16) ts.cnt[threadIdx.x] = 0;
     if (threadIdx.x < NBIN) ts.binhist[threadIdx.x] = 0;
+    if (threadIdx.x < NWARP) ts.raw_n[threadIdx.x] = 0;
     if (threadIdx.x == 0) {
         ts.n_quads = 0; ts.n_staged = 0; ts.flushed = 0; ts.elist_n = 0; ts.work = 0; ts.skip = 0;
     }

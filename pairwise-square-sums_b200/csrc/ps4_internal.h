@@ -74,7 +74,14 @@ struct SearchArgs {
     uint32_t flags;            // PS4_F_*
     uint32_t *jobs;            // 4-set job queue between gen_jobs and extend_jobs: 6 * jobs_cap u32 (SoA)
     uint64_t jobs_cap;
+    uint64_t *raw;             // optional (gen_jobs): per-CTA list of every representation of the tile,
+    uint32_t raw_cap;          //   raw_cap entries per CTA in NWARP equal warp slices
 };
+// representations a tile's raw list holds per CTA: (pi/8) * 2^14 = 6434 expected, 8192 with margin
+constexpr uint32_t RAW_PER_CTA = 8192;
+// the raw list pays from S ~ 1e10 up (measured on B200: 1.25x faster tile kernel at 1e11, break-even
+// at 1e10, slower below): the fill pass's rescan costs ~sqrt(S) steps per tile, recording ~W/3
+constexpr uint64_t RAW_MIN_S = 10000000000ull;
 
 // Arguments of one triple-extension launch (ps4_triples.cu).
 struct TriArgs {

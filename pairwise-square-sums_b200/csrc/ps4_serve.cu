@@ -268,6 +268,7 @@ struct ps4_server {
     cudaStream_t s_main = nullptr, s_tri = nullptr, s_post = nullptr, s_copy = nullptr;
     uint32_t *d_jobs = nullptr;
     uint64_t jobs_cap = 0;
+    uint64_t *d_raw = nullptr;               // per tile-kernel CTA representation lists
     uint32_t *d_scratch = nullptr;
     uint64_t scratch_words = 0;
     SlotDev *d_slots = nullptr;
@@ -591,6 +592,7 @@ int launch_step(ps4_server *s, StepBuf &b) {
         a.flags = s->v.flags & ~(uint32_t)PS4_F_DUMP4;
         a.jobs = s->d_jobs; a.jobs_cap = s->jobs_cap;
         if (!b.fused) {
+            a.raw = s->d_raw; a.raw_cap = RAW_PER_CTA;
             const int g = (int)std::min<uint64_t>((uint64_t)gen_grid(s->v.num_sms), std::max<uint64_t>(tiles, 1));
             SRV_CUDA(s, (cudaError_t)launch_gen(a, g, st));
             if (!(s->v.flags & PS4_F_NOEXT)) SRV_CUDA(s, (cudaError_t)launch_ext(a, ext_grid(s->v.num_sms), st));
@@ -937,6 +939,7 @@ extern "C" int ps4_serve_create(ps4_ctx *ctx, const ps4_serve_config *cfg, ps4_s
     s->jobs_cap = 1ull << 20;
     while (s->jobs_cap < (1ull << 27) && (double)s->jobs_cap < need) s->jobs_cap <<= 1;
     if (dev_alloc(s, s->d_jobs, 6 * s->jobs_cap)) return PS4_ERR_CUDA;
+    if (dev_alloc(s, s->d_raw, (uint64_t)gen_grid(s->v.num_sms) * RAW_PER_CTA)) return PS4_ERR_CUDA;
     if (dev_alloc(s, s->d_slots, c.max_slots)) return PS4_ERR_CUDA;
     for (int i = 0; i < 2; i++)
         if (init_buf(s, s->buf[i])) return PS4_ERR_CUDA;
@@ -960,7 +963,7 @@ extern "C" void ps4_serve_destroy(ps4_server *s) {
         cudaStreamSynchronize(s->s_copy);
     }
     for (int i = 0; i < 2; i++) free_buf(s->buf[i]);
-    cudaFree(s->d_jobs); cudaFree(s->d_scratch); cudaFree(s->d_slots); cudaFree(s->d_arena);
+    cudaFree(s->d_jobs); cudaFree(s->d_raw); cudaFree(s->d_scratch); cudaFree(s->d_slots); cudaFree(s->d_arena);
     for (cudaStream_t st : {s->s_main, s->s_tri, s->s_post, s->s_copy})
         if (st) cudaStreamDestroy(st);
     delete s;
