@@ -196,6 +196,7 @@ struct WarpArea {
     ExtEntry ext[EXCAP];
     uint32_t fp[FSLOT][32];              // each lane's primes of D, lane-minor (no bank conflicts)
     uint8_t fe[FSLOT][32];               //   and their exponents
+    uint32_t jsq[32];                    // ext_sqrt of each lane's 4-set in this warp batch
     uint32_t n_ext;
 };
 
@@ -505,6 +506,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
     const uint64_t njobs = min(*(volatile ull *)&a.status->n_jobs, (ull)a.jobs_cap);
     const uint64_t nbatch = (njobs + 31) >> 5;
     if (lane == 0) w->n_ext = 0;
+    w->jsq[lane] = 0;
     __syncwarp();
     LaneCounters cnt;
 
@@ -607,7 +609,6 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 jb = z.x & 0xFFFFu; L = z.x >> 16; H = z.y & 0xFFFFu; E2 = (z.y >> 16) & 0xFFu; flg = z.y >> 24;
                 R = (flg & 1) ? E2 - 1 : 1;
                 dlo = flg & 1; dhi = (flg & 1) ? E2 - 1 : 0;      // 2-exponents of f: [1, E2-1] or {0}
-                cnt.use(a, y.w);
                 cc = 0; l = 0; h = 0; d2 = (flg & 1) ? 1u : 0u;
             };
             if (g0 < g1) {
@@ -619,7 +620,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 l = to - h * L;
                 cc = cidx;
             }
-            uint32_t qn = 0;
+            uint32_t qn = 0, sq_run = 0;
             for (uint32_t it = 0; it < iters; it++) {
                 bool pass = false;
                 uint64_t u = 0;
@@ -642,7 +643,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                         const EJob &Ej = w->job[jcur];
                         if (e == A || e == Ej.B || e == Ej.C1 || e == Ej.C2) pass = false;
                     }
-                    if (pass) { cnt.sqrt_++; cidx = l | (h << 12) | (d2 << 24); }
+                    if (pass) { sq_run++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
                     {                                          // (l, h, d2) advance, branch-free
                         d2++;
@@ -654,6 +655,8 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                         h += wl;
                     }
                     if (++cc == ncand && it + 1 < g1 - g0) {
+                        if (sq_run) atomicAdd(&w->jsq[jl], sq_run);
+                        sq_run = 0;
                         do { jl++; } while (jl < 31 && w->cstart[jl + 1] == w->cstart[jl]);
                         load_job(jl);
                     }
@@ -673,10 +676,17 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     __syncwarp();
                 }
             }
+            if (sq_run) atomicAdd(&w->jsq[jl], sq_run);
             if (qn) process_queue(a, w, 0, qn, bbase, lane);
             __syncwarp();
             pending = pending && !fits;
         }
+        __syncwarp();
+        if (jidx < njobs) {                    // this lane's 4-set: its ext_sqrt into its item's counters
+            cnt.use(a, J.item);
+            cnt.sqrt_ += w->jsq[lane];
+        }
+        w->jsq[lane] = 0;
         __syncwarp();
         if (lane == 0 && w->n_ext) {
             report_warp_exts(a, w->ext, min(w->n_ext, (uint32_t)EXCAP));
