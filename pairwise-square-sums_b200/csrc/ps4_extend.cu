@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
 
 constexpr int EBS = 256;                 // threads per CTA
 constexpr int EWARPS = EBS / 32;
-constexpr int DCAP = 352;                // divisor-list entries per warp (u64)
+constexpr int DCAP = 416;                // divisor-list entries per warp (u64)
 constexpr int QCAP = 64;                 // square-test queue per warp
 constexpr int EXCAP = 8;                 // extensions per warp batch
 constexpr int FSLOT = 16;                // prime slots per lane: m1's primes from 0, m2's from 8
@@ -194,8 +194,8 @@ struct WarpArea {
     uint64_t qu[QCAP];
     uint8_t qj[QCAP];
     ExtEntry ext[EXCAP];
-    uint32_t fp[FSLOT][32];              // each lane's primes of D, lane-minor (no bank conflicts)
-    uint8_t fe[FSLOT][32];               //   and their exponents
+    uint32_t fp[FSLOT][32];              // each lane's primes of D with their exponents (p | e << 24),
+                                         //   lane-minor (no bank conflicts)
     uint32_t jsq[32];                    // ext_sqrt of each lane's 4-set in this warp batch
     uint32_t n_ext;
 };
@@ -355,7 +355,7 @@ struct LaneJob {
     uint32_t r[6], item;
     uint64_t v[4], S, A, C1, C2;
     int bi, bj, bk;
-    int np;                              // distinct primes, in w->fp/fe[0..np)[lane]
+    int np;                              // distinct primes, in w->fp[0..np)[lane]
     bool has2;
     int E2, j0, js;                      // odd primes are pr[j0..np); the high group starts at js
     uint32_t ndo, nd, ncand, L, H;
@@ -368,12 +368,11 @@ struct LaneJob {
 // list -- primes in first-seen order, as s4.c:141-147.  A new prime is written to a slot below
 // every unread slot of m2, so the merge is in place.
 __device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, uint32_t m2, uint32_t (*fp)[32],
-                                           uint8_t (*fe)[32], int lane) {
+                                           int lane) {
     int na = 0, nb = 0;
     if (m1 > 1 && !(m1 & 1)) {                      // both even
         const uint32_t z1 = (uint32_t)__ffs((int)m1) - 1, z2 = (uint32_t)__ffs((int)m2) - 1;
-        fp[0][lane] = 2;
-        fe[0][lane] = (uint8_t)(z1 + z2);
+        fp[0][lane] = 2u | ((z1 + z2) << 24);
         na = 1;
         m1 >>= z1;
         m2 >>= z2;
@@ -381,15 +380,13 @@ __device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, ui
     uint64_t sa = m1 > 1 ? __ldg(&spfq[m1]) : 0, sb = m2 > 1 ? __ldg(&spfq[m2]) : 0;
     while (m1 > 1 || m2 > 1) {
         if (m1 > 1) {
-            fp[na][lane] = spf_p(sa);
-            fe[na][lane] = (uint8_t)spf_e(sa);
+            fp[na][lane] = (uint32_t)sa;                   // p | e << 24, as the table stores it
             na++;
             m1 = spf_cof(sa);
             if (m1 > 1) sa = __ldg(&spfq[m1]);
         }
         if (m2 > 1) {
-            fp[8 + nb][lane] = spf_p(sb);
-            fe[8 + nb][lane] = (uint8_t)spf_e(sb);
+            fp[8 + nb][lane] = (uint32_t)sb;
             nb++;
             m2 = spf_cof(sb);
             if (m2 > 1) sb = __ldg(&spfq[m2]);
@@ -397,18 +394,17 @@ __device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, ui
     }
     int np = na;
     for (int j = 0; j < nb; j++) {
-        const uint32_t p = fp[8 + j][lane];
-        const uint8_t e = fe[8 + j][lane];
+        const uint32_t x = fp[8 + j][lane], p = x & 0xFFFFFFu;
         int i = 0;
-        while (i < na && fp[i][lane] != p) i++;
-        if (i < na) fe[i][lane] = (uint8_t)(fe[i][lane] + e);
-        else { fp[np][lane] = p; fe[np][lane] = e; np++; }
+        while (i < na && (fp[i][lane] & 0xFFFFFFu) != p) i++;
+        if (i < na) fp[i][lane] += x & 0xFF000000u;
+        else { fp[np][lane] = x; np++; }
     }
     return np;
 }
 
 __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJob &J, uint32_t (*fp)[32],
-                                          uint8_t (*fe)[32], int lane) {
+                                          int lane) {
     get_job(a.jobs, a.jobs_cap, j, J.r, J.item);
     quad_values(J.r, J.v, J.S);
     uint32_t best;
@@ -421,18 +417,18 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
         if (t != J.bi && t != J.bj) { if (o1 < 0) o1 = t; else o2 = t; }
     J.C1 = pick4(J.v, o1);
     J.C2 = pick4(J.v, o2);
-    J.np = factor_pair(a.spfq, ra - rb, ra + rb, fp, fe, lane);
+    J.np = factor_pair(a.spfq, ra - rb, ra + rb, fp, lane);
     // D even => both factors even => 2 is the first prime and 4 | D
-    J.has2 = J.np > 0 && fp[0][lane] == 2;
-    J.E2 = J.has2 ? fe[0][lane] : 0;
+    J.has2 = J.np > 0 && (fp[0][lane] & 0xFFFFFFu) == 2;
+    J.E2 = J.has2 ? fp[0][lane] >> 24 : 0;
     J.j0 = J.has2 ? 1 : 0;
     uint32_t ndo = 1;
-    for (int q = J.j0; q < J.np; q++) ndo *= (uint32_t)fe[q][lane] + 1;
+    for (int q = J.j0; q < J.np; q++) ndo *= (fp[q][lane] >> 24) + 1;
     J.ndo = ndo;
     // low group: the leading odd primes while their radix product stays <= sqrt(ndo)
     uint32_t L = 1, js = J.j0;
-    while (js < J.np && L * ((uint32_t)fe[js][lane] + 1) * L * ((uint32_t)fe[js][lane] + 1) <= ndo)
-        L *= (uint32_t)fe[js++][lane] + 1;
+    while (js < J.np && L * ((fp[js][lane] >> 24) + 1) * L * ((fp[js][lane] >> 24) + 1) <= ndo)
+        L *= (fp[js++][lane] >> 24) + 1;
     J.js = js;
     J.L = L;
     J.H = ndo / L;
@@ -445,12 +441,12 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
 }
 
 // divisors of prod pr[q]^ex[q], q in [q0, q1), in mixed-radix order (first prime fastest)
-__device__ __forceinline__ void gen_list(uint64_t *d, const uint32_t (*fp)[32], const uint8_t (*fe)[32], int lane,
+__device__ __forceinline__ void gen_list(uint64_t *d, const uint32_t (*fp)[32], int lane,
                                          int q0, int q1) {
     d[0] = 1;
     uint32_t nn = 1;
     for (int q = q0; q < q1; q++) {
-        const uint32_t cur = nn, pq = fp[q][lane], eq = fe[q][lane];
+        const uint32_t cur = nn, pq = fp[q][lane] & 0xFFFFFFu, eq = fp[q][lane] >> 24;
         uint64_t pk = 1;
         for (uint32_t e = 1; e <= eq; e++) {
             pk *= pq;
@@ -525,7 +521,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
 
         // ---- phase A: one 4-set per lane
         LaneJob J;
-        bool pending = jidx < njobs && job_setup(a, jidx, J, w->fp, w->fe, lane);
+        bool pending = jidx < njobs && job_setup(a, jidx, J, w->fp, lane);
         const bool big = pending && J.L + J.H > (uint32_t)DCAP;
         if (pending) {
             cnt.use(a, J.item);
@@ -548,8 +544,8 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             const uint32_t base = incl - want;
             const bool fits = pending && incl <= (uint32_t)DCAP;
             if (fits) {
-                gen_list(w->dbuf + base, w->fp, w->fe, lane, J.j0, J.js);              // lo: L entries
-                gen_list(w->dbuf + base + J.L, w->fp, w->fe, lane, J.js, J.np);        // hi: H entries
+                gen_list(w->dbuf + base, w->fp, lane, J.j0, J.js);              // lo: L entries
+                gen_list(w->dbuf + base + J.L, w->fp, lane, J.js, J.np);        // hi: H entries
                 EJob &E = w->job[lane];
                 E.A = J.A; E.C1 = J.C1; E.C2 = J.C2;
                 const int64_t dd1 = (int64_t)J.C1 - (int64_t)J.A, dd2 = (int64_t)J.C2 - (int64_t)J.A;
