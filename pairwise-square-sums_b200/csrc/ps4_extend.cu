@@ -4,14 +4,15 @@
 //                 4-set of the tile (P5: closed-form z ranges per representation pair) is
 //                 written to a global job queue: a count pass, one block scan, one atomic
 //                 reservation per tile, a write pass.                         (s4.c:280-341)
-//   extend_jobs   the extension engine.  A warp takes 32 queued 4-sets (one per lane).  Each
-//                 lane picks the difference to extend by, factors it and writes the odd part's
-//                 divisors, in the reference's mixed-radix order, into the warp's shared buffer.
-//                 Then the warp pools the candidates of all 32 4-sets -- the complementary
-//                 divisor pairs (f,g), f<g, of equal parity, each visited once -- and splits
-//                 them into 32 equal contiguous runs, one per lane, so every lane does the same
-//                 work whatever the divisor counts.  Residue filters mod 64/63/65 are bit tests
-//                 against per-4-set rotated residue masks; the candidates that pass (the
+//   extend_jobs   the extension engine.  Each lane of a warp holds one queued 4-set; it picks
+//                 the difference to extend by and factors it.  In rounds, the warp places the
+//                 factored odd-divisor lists of as many of its 4-sets as fit in its shared
+//                 buffer, pools the candidates of those 4-sets -- the complementary divisor
+//                 pairs (f,g), f<g, of equal parity, each visited once -- and splits them into
+//                 32 equal contiguous runs, one per lane, so every lane does the same work
+//                 whatever the divisor counts; lanes whose 4-set is done take the next one from
+//                 the queue before the next round.  Residue filters mod 64/63/65 are bit tests
+//                 against per-4-set masks indexed by u's residue; the candidates that pass (the
 //                 reference's ext_sqrt) go through a warp queue and are square-tested 32 at a
 //                 time.                                                        (s4.c:160-207)
 //
@@ -196,7 +197,8 @@ struct WarpArea {
     ExtEntry ext[EXCAP];
     uint32_t fp[FSLOT][32];              // each lane's primes of D with their exponents (p | e << 24),
                                          //   lane-minor (no bank conflicts)
-    uint32_t jsq[32];                    // ext_sqrt of each lane's 4-set in this warp batch
+    uint32_t jsq[32];                    // ext_sqrt of each lane's 4-set in this round
+    uint32_t jid[32];                    // queue index of each lane's 4-set
     uint32_t n_ext;
 };
 
@@ -465,7 +467,7 @@ static __device__ __noinline__ void extend_big(const SearchArgs &a, const LaneJo
 // Square tests of queue entries [first, first+count), one per lane (s4.c:199-203); a hit
 // gets its order key, the reference's mixed-radix index of the smaller divisor.
 __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, uint32_t first, uint32_t count,
-                                              uint64_t bbase, int lane) {
+                                              int lane) {
     if ((uint32_t)lane < count) {
         const uint32_t idx = first + lane;
         const uint64_t u = w->qu[idx];
@@ -483,7 +485,7 @@ __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, 
             const uint32_t slot = atomicAdd(&w->n_ext, 1u);
             if (slot < EXCAP) {
                 ExtEntry &x = w->ext[slot];
-                x.qid = (uint32_t)(bbase + jl);
+                x.qid = w->jid[jl];
                 x.key = key;
                 x.lo = (uint64_t)e;
                 x.hi = (uint64_t)(e >> 64);
@@ -500,49 +502,67 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
     WarpArea *w = (WarpArea *)(esmem + (size_t)wid * sizeof(WarpArea));
     const unsigned FULL = 0xffffffffu;
     const uint64_t njobs = min(*(volatile ull *)&a.status->n_jobs, (ull)a.jobs_cap);
-    const uint64_t nbatch = (njobs + 31) >> 5;
     if (lane == 0) w->n_ext = 0;
     w->jsq[lane] = 0;
     __syncwarp();
     LaneCounters cnt;
+    LaneJob J;
+    bool pending = false, old = false, drained = false;
+    uint32_t myjob = 0;
 
+    // Rolling rounds: before each round every lane without a 4-set takes the next one from the
+    // queue (phase A), so every round runs with a full warp of 4-sets; a lane whose divisor
+    // lists did not fit keeps its 4-set and goes first in the next round's placement.
     for (;;) {
-        uint32_t b = 0;
-        int stop = 0;
-        if (lane == 0) {
-            b = atomicAdd(&a.status->ext_next, 1u);
-            stop = *(volatile ull *)&a.status->err != 0ull;
+        if (!drained) {
+            const bool need = !pending;
+            const unsigned m = __ballot_sync(FULL, need);
+            uint32_t base = 0;
+            int stop = 0;
+            if (lane == 0) {
+                if (m) base = atomicAdd(&a.status->ext_next, (uint32_t)__popc(m));
+                stop = *(volatile ull *)&a.status->err != 0ull;
+            }
+            base = __shfl_sync(FULL, base, 0);
+            stop = __shfl_sync(FULL, stop, 0);
+            if (stop) break;                                             // warp-uniform
+            if ((uint64_t)base + __popc(m) >= njobs) drained = true;     // warp-uniform
+            if (need) {
+                const uint64_t jidx = (uint64_t)base + __popc(m & ((1u << lane) - 1u));
+                if (jidx < njobs) {
+                    myjob = (uint32_t)jidx;
+                    old = false;
+                    // ---- phase A: one 4-set per lane
+                    pending = job_setup(a, jidx, J, w->fp, lane);
+                    const bool big = pending && J.L + J.H > (uint32_t)DCAP;
+                    if (pending) {
+                        cnt.use(a, J.item);
+                        if (J.nd > cnt.mdiv) cnt.mdiv = J.nd;
+                        if (!big) cnt.cand += J.ncand;
+                    }
+                    if (big) {               // extremely rare: its factored lists exceed the buffer
+                        extend_big(a, J, myjob, cnt.cand, cnt.sqrt_, w->ext, &w->n_ext);
+                        pending = false;
+                    }
+                }
+            }
         }
-        b = __shfl_sync(FULL, b, 0);
-        stop = __shfl_sync(FULL, stop, 0);
-        if (b >= nbatch || stop) break;                                  // warp-uniform
-        const uint64_t bbase = (uint64_t)b << 5;
-        const uint64_t jidx = bbase + lane;
-
-        // ---- phase A: one 4-set per lane
-        LaneJob J;
-        bool pending = jidx < njobs && job_setup(a, jidx, J, w->fp, lane);
-        const bool big = pending && J.L + J.H > (uint32_t)DCAP;
-        if (pending) {
-            cnt.use(a, J.item);
-            if (J.nd > cnt.mdiv) cnt.mdiv = J.nd;
-            if (!big) cnt.cand += J.ncand;
-        }
-        if (big) {                       // extremely rare: its factored lists exceed the buffer
-            extend_big(a, J, (uint32_t)jidx, cnt.cand, cnt.sqrt_, w->ext, &w->n_ext);
-            pending = false;
-        }
-        while (__any_sync(FULL, pending)) {
-            // place the factored divisor lists of as many pending lanes as fit, in lane order
+        const bool round = __any_sync(FULL, pending);
+        if (round) {
+            // place the factored divisor lists of as many pending lanes as fit: lanes left over
+            // from the last round first, then the new ones, each in lane order
             const uint32_t want = pending ? J.L + J.H : 0;
-            uint32_t incl = want;
+            uint32_t io = old ? want : 0, in = old ? 0 : want;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(FULL, incl, o);
-                if (lane >= o) incl += y;
+                const uint32_t yo = __shfl_up_sync(FULL, io, o), yn = __shfl_up_sync(FULL, in, o);
+                if (lane >= o) { io += yo; in += yn; }
             }
+            const uint32_t tot_old = __shfl_sync(FULL, io, 31);           // every lane takes part
+            const uint32_t incl = old ? io : tot_old + in;
             const uint32_t base = incl - want;
             const bool fits = pending && incl <= (uint32_t)DCAP;
+            if (fits) w->jid[lane] = myjob;
             if (fits) {
                 gen_list(w->dbuf + base, w->fp, lane, J.j0, J.js);              // lo: L entries
                 gen_list(w->dbuf + base + J.L, w->fp, lane, J.js, J.np);        // hi: H entries
@@ -667,28 +687,29 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 qn += __popc(m);
                 __syncwarp();
                 if (qn >= 32) {
-                    process_queue(a, w, qn - 32, 32, bbase, lane);
+                    process_queue(a, w, qn - 32, 32, lane);
                     qn -= 32;
                     __syncwarp();
                 }
             }
             if (sq_run) atomicAdd(&w->jsq[jl], sq_run);
-            if (qn) process_queue(a, w, 0, qn, bbase, lane);
+            if (qn) process_queue(a, w, 0, qn, lane);
             __syncwarp();
+            if (fits) {                        // this lane's 4-set is done: its ext_sqrt into its item
+                cnt.use(a, J.item);
+                cnt.sqrt_ += w->jsq[lane];
+                w->jsq[lane] = 0;
+            }
             pending = pending && !fits;
+            old = pending;
         }
         __syncwarp();
-        if (jidx < njobs) {                    // this lane's 4-set: its ext_sqrt into its item's counters
-            cnt.use(a, J.item);
-            cnt.sqrt_ += w->jsq[lane];
-        }
-        w->jsq[lane] = 0;
-        __syncwarp();
-        if (lane == 0 && w->n_ext) {
+        if (lane == 0 && w->n_ext) {          // this round's extensions (and any from the per-lane path)
             report_warp_exts(a, w->ext, min(w->n_ext, (uint32_t)EXCAP));
             w->n_ext = 0;
         }
         __syncwarp();
+        if (!round && drained) break;          // warp-uniform
     }
     cnt.flush(a);
 }
