@@ -53,23 +53,12 @@ __device__ __forceinline__ void get_job(const uint32_t *jobs, uint64_t cap, uint
 
 // ================================================================== gen_jobs
 
-// The 4-sets of representation pair gidx of the tile (P5).  Counts them; with WRITE also
-// builds, checks, dumps and (when `store`) queues them at out, out+1, ...
+// The 4-sets of representation pair gidx of the tile (P5), pair given as list s and (x, y).
+// Counts them; with WRITE also builds, checks, dumps and (when `store`) queues them at out, ...
 template <bool WRITE>
-__device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t gidx, uint32_t nI,
-                                               const uint16_t *is_off, const uint16_t *is_k,
-                                               const uint16_t *is_start, const uint32_t *is_pbase,
-                                               const uint32_t *rep_p, const uint32_t *rep_q, uint64_t S0,
-                                               uint32_t item, uint64_t out, bool store) {
-    uint32_t lo = 0, hi = nI;
-    while (hi - lo > 1) {
-        const uint32_t mid = (lo + hi) >> 1;
-        if (is_pbase[mid] <= gidx) lo = mid; else hi = mid;
-    }
-    const uint32_t st = is_start[lo], k = is_k[lo];
-    const uint64_t S = S0 + is_off[lo];
-    uint32_t x, y;
-    decode_pair(gidx - is_pbase[lo], x, y);
+__device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t st, uint32_t k, uint64_t S,
+                                               uint32_t x, uint32_t y, const uint32_t *rep_p,
+                                               const uint32_t *rep_q, uint32_t item, uint64_t out, bool store) {
     const uint32_t px = rep_p[st + x], py = rep_p[st + y];
     const uint64_t Px = (uint64_t)px * px, Py = (uint64_t)py * py;
     const uint32_t pxy = (px + py) & 1;
@@ -104,6 +93,32 @@ __device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t gid
     return n;
 }
 
+// A lane's share of P5: the pairs g = gw + lane, gw + lane + 32, ... below ge of its warp's
+// contiguous block.  Neighbouring lanes take neighbouring pairs (mostly the same S), and each
+// lane finds its pair's S by one binary search, then by stepping forward.
+template <bool WRITE>
+__device__ __forceinline__ uint32_t lane_pairs(const SearchArgs &a, uint32_t gw, uint32_t ge, int lane, uint32_t nI,
+                                               const uint16_t *is_off, const uint16_t *is_k,
+                                               const uint16_t *is_start, const uint32_t *is_pbase,
+                                               const uint32_t *rep_p, const uint32_t *rep_q, uint64_t S0,
+                                               uint32_t item, uint64_t out, bool store) {
+    uint32_t g = gw + (uint32_t)lane;
+    if (g >= ge) return 0;
+    uint32_t lo = 0, hi = nI;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (is_pbase[mid] <= g) lo = mid; else hi = mid;
+    }
+    uint32_t n = 0;
+    for (; g < ge; g += 32) {
+        while (lo + 1 < nI && is_pbase[lo + 1] <= g) lo++;
+        uint32_t x, y;
+        decode_pair(g - is_pbase[lo], x, y);
+        n += pair_quads<WRITE>(a, is_start[lo], is_k[lo], S0 + is_off[lo], x, y, rep_p, rep_q, item, out + n, store);
+    }
+    return n;
+}
+
 template <int TL>
 __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
     using L = TileLayout<TL>;
@@ -134,9 +149,12 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
         const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
         const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
         // count pass, one reservation for the tile, write pass in the same order
-        uint32_t mine = 0;
-        for (uint32_t g = tid; g < nPairs; g += BS)
-            mine += pair_quads<false>(a, g, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item, 0, false);
+        // each warp a contiguous block of pairs (whole multiples of 32)
+        const int lane = tid & 31, wid = tid >> 5;
+        const uint32_t blk = ((nPairs + NWARP * 32 - 1) / (NWARP * 32)) * 32;
+        const uint32_t gw = (uint32_t)wid * blk, ge = min(nPairs, gw + blk);
+        uint32_t mine = lane_pairs<false>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0,
+                                          item, 0, false);
         uint32_t off, d1, d2, tot[3];
         block_scan3(mine, 0u, 0u, off, d1, d2, tot, ts.wsum);
         if (tid == 0) {
@@ -152,9 +170,8 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
         __syncthreads();
         if (need_write_pass) {
             const bool store = s_store != 0;
-            uint64_t pos = s_base + off;
-            for (uint32_t g = tid; g < nPairs; g += BS)
-                pos += pair_quads<true>(a, g, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item, pos, store);
+            lane_pairs<true>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item,
+                             s_base + off, store);
         }
         __syncthreads();
         tile_flush_counters(a, ts, item);
