@@ -311,6 +311,12 @@ uint64_t ps4_last_launches(const ps4_ctx *ctx);
  * extension order -- into buf, NUL-terminated (s4.c:247-269, format_set s4.c:214-220).
  * Returns the length, or -1 if cap is too small.  `exts` is the results' ext array. */
 long ps4_format_hit(const ps4_hit *hit, const ps4_ext *exts, char *buf, size_t cap);
+/* ps4_format_hit's lines of hits[0..n) concatenated into buf (NUL-terminated), and the query
+ * item of each line into line_items (may be NULL; at most n + the hits' extension count lines).
+ * Returns the length, or -(length needed + 1) when cap is too small (then nothing past the
+ * last complete hit is written and line_items stops there too); *n_lines gets the line count. */
+long ps4_format_hits(const ps4_hit *hits, uint64_t n, const ps4_ext *exts, char *buf, size_t cap,
+                     uint32_t *line_items, uint64_t *n_lines);
 /* The "!!!!!!!! FOUND 6-SET:" alert line of a 6-set record (s4.c:270-276).  Returns length or -1. */
 long ps4_format_six(const ps4_hit *hit, const ps4_ext *exts, const ps4_six *six, char *buf, size_t cap);
 /* The --test-sixset drill line for an M hit (s4.c:255-260).  Returns length or -1. */

@@ -78,6 +78,35 @@ long ps4_format_hit(const ps4_hit *h, const ps4_ext *exts, char *buf, size_t cap
     return done(&b);
 }
 
+long ps4_format_hits(const ps4_hit *hits, uint64_t n, const ps4_ext *exts, char *buf, size_t cap,
+                     uint32_t *line_items, uint64_t *n_lines) {
+    char tmp[8192];
+    size_t len = 0;
+    uint64_t lines = 0;
+    int full = 0;
+    if (cap) buf[0] = 0;
+    for (uint64_t i = 0; i < n; i++) {
+        char *dst = full ? tmp : buf + len;
+        size_t room = full ? sizeof tmp : cap - len;
+        long k = ps4_format_hit(&hits[i], exts, dst, room);
+        if (k < 0 && !full) {                  /* buf is too small: keep counting the length */
+            full = 1;
+            if (len < cap) buf[len] = 0;       /* end at the last complete hit */
+            k = ps4_format_hit(&hits[i], exts, tmp, sizeof tmp);
+            dst = tmp;
+        }
+        if (k < 0) return -1;                  /* a single hit longer than 8 KB: not produced by a search */
+        for (long c = 0; c < k; c++)
+            if (dst[c] == '\n') {
+                if (line_items && !full) line_items[lines] = hits[i].item;
+                lines++;
+            }
+        len += (size_t)k;
+    }
+    if (n_lines) *n_lines = lines;
+    return full ? -(long)(len + 1) : (long)len;
+}
+
 long ps4_format_six(const ps4_hit *h, const ps4_ext *exts, const ps4_six *s, char *buf, size_t cap) {
     sbuf b = {buf, cap, 0, cap == 0};
     if (cap) buf[0] = 0;

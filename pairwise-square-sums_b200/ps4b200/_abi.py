@@ -146,6 +146,8 @@ def load() -> C.CDLL:
         "ps4_graph_counts": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
         "ps4_last_kernel_split": (None, [C.c_void_p, P(C.c_double), P(C.c_double)]),
         "ps4_format_hit": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),
+        "ps4_format_hits": (C.c_long, [P(Hit), C.c_uint64, P(Ext), C.c_char_p, C.c_size_t, P(C.c_uint32),
+                                       P(C.c_uint64)]),
         "ps4_format_six": (C.c_long, [P(Hit), P(Ext), P(Six), C.c_char_p, C.c_size_t]),
         "ps4_format_drill": (C.c_long, [P(Hit), P(Ext), C.c_char_p, C.c_size_t]),
         "ps4_format_quad": (C.c_long, [P(Quad), C.c_char_p, C.c_size_t]),

@@ -257,13 +257,21 @@ class Search:
     def _collect(self, out: RangeResult):
         r = self._res
         buf = C.create_string_buffer(_LINE_CAP)
-        for i in range(r.n_hits):
-            h = C.byref(self._hits[i])
-            n = self.lib.ps4_format_hit(h, self._exts, buf, _LINE_CAP)
-            if n > 0:
-                for line in buf.value.decode().splitlines(keepends=True):
-                    out.lines.append(line)
-                    out.items.append(self._hits[i].item)
+        if r.n_hits:
+            # every hit's lines in one call (ps4_format_hits), grown once if the estimate is short
+            cap = max(1 << 16, 160 * r.n_hits + 48 * r.n_exts)
+            items = (C.c_uint32 * (r.n_hits + r.n_exts))()
+            nl = C.c_uint64()
+            for _ in range(2):
+                big = C.create_string_buffer(cap)
+                n = self.lib.ps4_format_hits(self._hits, r.n_hits, self._exts, big, cap, items, C.byref(nl))
+                if n >= 0:
+                    break
+                if n == -1:
+                    raise Ps4Error(_abi.PS4_ERR_ARG, "a hit formats to more than 8 KB")
+                cap = -n
+            out.lines.extend(big.raw[:n].decode().splitlines(keepends=True))
+            out.items.extend(items[:nl.value])
         for s in range(r.n_sixes):
             six = self._sixes[s]
             n = self.lib.ps4_format_six(C.byref(self._hits[six.hit]), self._exts, C.byref(six), buf, _LINE_CAP)

@@ -1,0 +1,58 @@
+"""Host line formatting (ps4_format_*, csrc/ps4_format.c): the batch formatter equals the
+per-hit one, line for line, on synthetic records (no GPU)."""
+from __future__ import annotations
+
+import ctypes as C
+import random
+
+from ps4b200 import _abi
+
+
+def _records(n, seed):
+    rng = random.Random(seed)
+    hits = (_abi.Hit * n)()
+    exts = []
+    for i in range(n):
+        h = hits[i]
+        h.S = rng.randrange(10 ** 6, 10 ** 12)
+        for j in range(4):
+            h.v[j] = rng.randrange(1, h.S)
+        k = rng.choice([1, 1, 2, 3])
+        h.n_ext, h.first_ext, h.item = k, len(exts), rng.randrange(0, 50)
+        h.flags = _abi.PS4_HIT_MULTI if k >= 2 else 0
+        for _ in range(k):
+            e = _abi.Ext()
+            e.lo = rng.randrange(1, 2 ** 64)
+            e.hi = rng.choice([0, 0, 0, rng.randrange(1, 2 ** 20)])
+            e.flags = rng.choice([0, _abi.PS4_EXT_FIVE, _abi.PS4_EXT_FIVE | _abi.PS4_EXT_FIVE_OK])
+            exts.append(e)
+    earr = (_abi.Ext * max(len(exts), 1))(*exts)
+    return hits, earr, len(exts)
+
+
+def test_batch_formatter_matches_per_hit():
+    lib = _abi.load()
+    hits, exts, ne = _records(500, 3)
+    want_lines, want_items = [], []
+    buf = C.create_string_buffer(1 << 14)
+    for i in range(len(hits)):
+        n = lib.ps4_format_hit(C.byref(hits[i]), exts, buf, len(buf))
+        assert n >= 0
+        for line in buf.value.decode().splitlines(keepends=True):
+            want_lines.append(line)
+            want_items.append(hits[i].item)
+    assert len(want_lines) > 300
+    cap = 1 << 20
+    big = C.create_string_buffer(cap)
+    items = (C.c_uint32 * (len(hits) + ne))()
+    nl = C.c_uint64()
+    n = lib.ps4_format_hits(hits, len(hits), exts, big, cap, items, C.byref(nl))
+    assert n == sum(len(x) for x in want_lines)
+    assert big.raw[:n].decode().splitlines(keepends=True) == want_lines
+    assert nl.value == len(want_lines) and list(items[:nl.value]) == want_items
+    # too small: the needed length comes back, the buffer ends at a complete hit
+    small = C.create_string_buffer(1000)
+    n2 = lib.ps4_format_hits(hits, len(hits), exts, small, 1000, None, C.byref(nl))
+    assert n2 == -(n + 1) and nl.value == len(want_lines)
+    got = small.value.decode()
+    assert got == "".join(want_lines)[:len(got)] and got.endswith("\n") and len(got) < 1000
