@@ -41,9 +41,21 @@ METRIC = "range_per_s"
 UNIT = "S/s"
 
 
-def shard(rank: int) -> tuple[int, int]:
+def shard(rank: int, bound: int = BOUND) -> tuple[int, int]:
     """Rank r searches S in [max(1, r*B), (r+1)*B): rank 0 is the s4 bound-1e10 workload."""
-    return max(1, rank * BOUND), (rank + 1) * BOUND
+    return max(1, rank * bound), (rank + 1) * bound
+
+
+def aggregate(dist, world: int, times: list, totals: list, device) -> tuple[list, list]:
+    """The job's figures from every rank's: the slowest rank's times (max), the summed totals.
+    The only collectives of a multi-GPU run; the search itself exchanges nothing."""
+    import torch
+    vals = torch.tensor(times, dtype=torch.float64, device=device)
+    tot = torch.tensor(totals, dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    return vals.tolist(), tot.tolist()
 
 
 # ------------------------------------------------------------------ CPU reference (s4)
@@ -426,13 +438,8 @@ def main():
         sk.finish(want_lines=False)
         gen_ms, ext_ms = sk.last_kernel_split
 
-    vals = torch.tensor([dev_s, e2e_s, kern_s], dtype=torch.float64, device="cuda")
-    tot = torch.tensor([S_rank, cand_rank], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-        dist.all_reduce(tot, op=dist.ReduceOp.SUM)
-    dev_s, e2e_s, kern_s = vals.tolist()
-    S_all, cand_all = tot.tolist()
+    (dev_s, e2e_s, kern_s), (S_all, cand_all) = aggregate(dist, world, [dev_s, e2e_s, kern_s],
+                                                          [S_rank, cand_rank], "cuda")
 
     plain = None
     if world == 1 and args.kernel == "batched" and not args.no_plain:
