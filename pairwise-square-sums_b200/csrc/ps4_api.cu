@@ -50,7 +50,7 @@ struct ps4_ctx {
     uint64_t last_launches = 0;
     unsigned tile_log2 = 14;             // current tile size (may shrink on E_TILE)
     PendingSearch pend;
-    uint64_t *d_raw = nullptr;           // per tile-kernel CTA: the tile's representations (RAW_PER_CTA)
+    uint64_t *d_raw = nullptr;           // per tile-kernel CTA: SUPER_K tile lists of RAW_PER_TILE
     uint64_t raw_words = 0;
     uint32_t *d_jobs = nullptr;          // 4-set job queue of the two-kernel pipeline (6 x jobs_cap u32)
     uint64_t jobs_cap = 1ull << 20;          // grows with the calls, up to 2^27 (3.2 GB)
@@ -352,8 +352,9 @@ static int enqueue_items(ps4_ctx *c) {
     }
     if (kernel == PS4_KERNEL_BATCHED && c->d_jobs_words < 6 * c->jobs_cap)
         if (grow(c, c->d_jobs, c->d_jobs_words, 6 * c->jobs_cap)) return PS4_ERR_CUDA;
-    if (kernel == PS4_KERNEL_BATCHED && c->raw_words < (uint64_t)c->num_sms * c->gen_ctas * RAW_PER_CTA)
-        if (grow(c, c->d_raw, c->raw_words, (uint64_t)c->num_sms * 2 * RAW_PER_CTA)) return PS4_ERR_CUDA;
+    if (kernel == PS4_KERNEL_BATCHED &&
+        c->raw_words < (uint64_t)c->num_sms * c->gen_ctas * SUPER_K * RAW_PER_TILE)
+        if (grow(c, c->d_raw, c->raw_words, (uint64_t)c->num_sms * 2 * SUPER_K * RAW_PER_TILE)) return PS4_ERR_CUDA;
     const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
     int grid = c->num_sms * (c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1);
     if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
@@ -377,7 +378,7 @@ static int enqueue_items(ps4_ctx *c) {
     a.flags = c->cfg.flags & (p.dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
     a.jobs = c->d_jobs;
     a.jobs_cap = c->jobs_cap;
-    if (kernel == PS4_KERNEL_BATCHED) { a.raw = c->d_raw; a.raw_cap = RAW_PER_CTA; }
+    if (kernel == PS4_KERNEL_BATCHED) { a.raw = c->d_raw; a.raw_cap = RAW_PER_TILE; }
     const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
     const int g_gen = c->num_sms * (int)c->gen_ctas, g_ext = c->num_sms * (int)c->ext_ctas;
 

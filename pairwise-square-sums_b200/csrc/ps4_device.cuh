@@ -335,7 +335,6 @@ struct TileShared {
     uint32_t elist_n, work;
     uint32_t binhist[NBIN], binstart[NBIN];
     uint32_t skip;             // tile abandoned (error)
-    uint32_t raw_n[NWARP];     // representations each warp appended to the tile's raw list
     uint64_t tile;
 };
 
@@ -388,8 +387,7 @@ __device__ __forceinline__ uint32_t isqrt_lt2p46(uint64_t x) {
 // ceil(sqrt(S0-q^2)) by a float estimate with exact integer correction (S < 2^44).
 template <bool FILL>
 __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t *cnt32, uint32_t *rep_p,
-                                              uint32_t *rep_q, uint64_t *raw = nullptr, uint32_t *raw_n = nullptr,
-                                              uint32_t slice = 0) {
+                                              uint32_t *rep_q) {
     const uint64_t S1 = S0 + n;
     uint32_t qmin = (uint32_t)ceil_sqrt64((S0 + 1) >> 1);
     if (qmin < 1) qmin = 1;
@@ -408,15 +406,6 @@ __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t 
             if (!FILL) {
                 atomicAdd(&cnt32[w], 1u << sh);
                 found++;
-                if (raw) {                                 // warp-aggregated append to this warp's slice
-                    const unsigned am = __activemask();
-                    const int lane = threadIdx.x & 31, lead = __ffs(am) - 1;
-                    uint32_t base = 0;
-                    if (lane == lead) base = atomicAdd(raw_n, (uint32_t)__popc(am));
-                    base = __shfl_sync(am, base, lead);
-                    const uint32_t pos = base + __popc(am & ((1u << lane) - 1u));
-                    if (pos < slice) raw[pos] = (uint64_t)i | ((uint64_t)p << 14) | ((uint64_t)q << 36);
-                }
             } else {
                 const uint32_t cur = (((volatile uint32_t *)cnt32)[w] >> sh) & 0xFFFFu;
                 if (cur == 0xFFFFu) continue;          // S not selected
@@ -429,9 +418,42 @@ __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t 
     return found;
 }
 
-// P1-P4 for one tile.  Returns false if the tile was abandoned (error raised).
+// The scan of scan_reps over a group of up to SUPER_K adjacent tiles [SS0, SS1) of one
+// segment, done once: every representation goes to its tile's list (offset in the tile | p << 14 |
+// q << 36; p <= q < 2^22, offset < 2^14), in the slice of the warp that found it (one shared
+// atomic per representation).  Slice counts above `slice` mean the list overflowed; that tile
+// then scans for itself.
+__device__ __forceinline__ void scan_group(uint64_t SS0, uint64_t SS1, unsigned TLv, uint64_t *lists,
+                                           uint32_t list_cap, uint32_t *raw_n, uint32_t slice) {
+    uint32_t qmin = (uint32_t)ceil_sqrt64((SS0 + 1) >> 1);
+    if (qmin < 1) qmin = 1;
+    const uint32_t qmax = SS1 >= 2 ? (uint32_t)isqrt64(SS1 - 2) : 0;
+    const int wid = threadIdx.x >> 5;
+    const uint32_t wmask = (1u << TLv) - 1u;
+    for (uint32_t q = qmin + threadIdx.x; q <= qmax; q += BS) {
+        const uint64_t q2 = (uint64_t)q * q;
+        uint32_t p = 1;
+        if (SS0 > q2 + 1) {
+            const uint64_t m = SS0 - q2;
+            const uint32_t r = isqrt_lt2p46(m);
+            p = r + ((uint64_t)r * r < m ? 1u : 0u);
+        }
+        for (uint64_t s = (uint64_t)p * p + q2; p <= q && s < SS1; s += 2 * p + 1, p++) {
+            const uint32_t i = (uint32_t)(s - SS0), j = i >> TLv;
+            const uint32_t pos = atomicAdd(&raw_n[j * NWARP + wid], 1u);
+            if (pos < slice)
+                lists[(size_t)j * list_cap + (size_t)wid * slice + pos] =
+                    (uint64_t)(i & wmask) | ((uint64_t)p << 14) | ((uint64_t)q << 36);
+        }
+    }
+}
+
+// P1-P4 for one tile.  Returns false if the tile was abandoned (error raised).  With `list` (the
+// tile's representations from scan_group, list_n[w] entries in warp slice w of `slice`) P1 and
+// P3 read the list; without, they scan.
 template <int TL>
-__device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *smem, uint64_t S0, uint32_t n) {
+__device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *smem, uint64_t S0, uint32_t n,
+                          const uint64_t *list = nullptr, const uint32_t *list_n = nullptr, uint32_t slice = 0) {
     using L = TileLayout<TL>;
     uint32_t *cnt32 = (uint32_t *)(smem + L::OFF_CNT);
     uint16_t *is_off = (uint16_t *)(smem + L::OFF_IS_OFF);
@@ -444,12 +466,20 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
 
     for (uint32_t i = tid; i < L::W / 2; i += BS) cnt32[i] = 0;
     __syncthreads();
-    // P1: count -- and, given a raw list and a tile from RAW_MIN_S up, record every representation
-    // (p <= q < 2^22, offset < 2^14) so that P3 need not scan again
-    const bool use_raw = a.raw != nullptr && S0 >= RAW_MIN_S;
-    const uint32_t slice = use_raw ? a.raw_cap / NWARP : 0;
-    uint64_t *raw_w = use_raw ? a.raw + (size_t)blockIdx.x * a.raw_cap + (size_t)(tid >> 5) * slice : nullptr;
-    const uint32_t found = scan_reps<false>(S0, n, cnt32, rep_p, rep_q, raw_w, &ts.raw_n[tid >> 5], slice);
+    // P1: count, from the list or by scanning
+    uint32_t found = 0;
+    if (list) {
+        for (int w = 0; w < NWARP; w++) {
+            const uint32_t cw = list_n[w];
+            for (uint32_t o = tid; o < cw; o += BS) {
+                const uint32_t i = (uint32_t)list[(size_t)w * slice + o] & 0x3FFFu;
+                atomicAdd(&cnt32[i >> 1], 1u << ((i & 1) * 16));
+                found++;
+            }
+        }
+    } else {
+        found = scan_reps<false>(S0, n, cnt32, rep_p, rep_q);
+    }
     ull f = warp_sum((ull)found);
     if ((tid & 31) == 0 && f) atomicAdd(&ts.cnt[K_PAIRS], f);
     __syncthreads();
@@ -513,15 +543,12 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
         cnt32[i >> 1] = word;
     }
     __syncthreads();
-    // P3: fill, from the raw list when every warp's slice held its representations
-    bool from_raw = use_raw;
-    for (int w = 0; w < NWARP; w++) from_raw = from_raw && ts.raw_n[w] <= slice;
-    if (from_raw) {
-        const uint64_t *raw = a.raw + (size_t)blockIdx.x * a.raw_cap;
+    // P3: fill, from the list or by scanning again
+    if (list) {
         for (int w = 0; w < NWARP; w++) {
-            const uint32_t cw = ts.raw_n[w];
+            const uint32_t cw = list_n[w];
             for (uint32_t o = tid; o < cw; o += BS) {
-                const uint64_t e = raw[(size_t)w * slice + o];
+                const uint64_t e = list[(size_t)w * slice + o];
                 const uint32_t i = (uint32_t)e & 0x3FFFu, wd = i >> 1, sh = (i & 1) * 16;
                 const uint32_t cur = (((volatile uint32_t *)cnt32)[wd] >> sh) & 0xFFFFu;
                 if (cur == 0xFFFFu) continue;          // S not selected
@@ -677,7 +704,6 @@ __device__ __forceinline__ void tile_flush_counters(const SearchArgs &a, TileSha
 __device__ __forceinline__ void tile_reset(TileShared &ts) {
     if (threadIdx.x < 16) ts.cnt[threadIdx.x] = 0;
     if (threadIdx.x < NBIN) ts.binhist[threadIdx.x] = 0;
-    if (threadIdx.x < NWARP) ts.raw_n[threadIdx.x] = 0;
     if (threadIdx.x == 0) {
         ts.n_quads = 0; ts.n_staged = 0; ts.flushed = 0; ts.elist_n = 0; ts.work = 0; ts.skip = 0;
     }

@@ -129,53 +129,94 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
     const int tid = threadIdx.x;
     const bool noext = (a.flags & PS4_F_NOEXT) != 0;
     const bool need_write_pass = !noext || (a.flags & (PS4_F_DUMP4 | PS4_F_VERIFY));
+    __shared__ unsigned long long s_claim;
+    uint64_t *lists = a.raw ? a.raw + (size_t)blockIdx.x * SUPER_K * a.raw_cap : nullptr;
+    // per tile of a group and warp: representations appended to the tile's list; in the tile
+    // layout's extension-list area, which this kernel does not use otherwise
+    uint32_t *raw_n = (uint32_t *)(smem + L::OFF_ELIST);
+    const uint32_t slice = a.raw ? a.raw_cap / NWARP : 0;
     for (;;) {
-        tile_reset(ts);
+        // claim SUPER_K tiles; tiles are taken from the last one down (costliest first)
         if (tid == 0) {
-            ts.tile = atomicAdd(&a.status->tile_next, 1u);
+            s_claim = atomicAdd(&a.status->tile_next, SUPER_K);
             ts.skip = *(volatile ull *)&a.status->err != 0ull;
         }
         __syncthreads();
-        if (ts.tile >= a.n_tiles || ts.skip) break;                      // block-uniform
-        uint32_t item, n;
-        uint64_t S0;
-        tile_bounds(a, ts.tile, TL, item, S0, n);
-        if (!tile_reps<TL>(a, ts, smem, S0, n)) { __syncthreads(); continue; }
-        const uint16_t *is_off = (const uint16_t *)(smem + L::OFF_IS_OFF);
-        const uint16_t *is_k = (const uint16_t *)(smem + L::OFF_IS_K);
-        const uint16_t *is_start = (const uint16_t *)(smem + L::OFF_IS_START);
-        const uint32_t *is_pbase = (const uint32_t *)(smem + L::OFF_IS_PBASE);
-        const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
-        const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
-        const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
-        // count pass, one reservation for the tile, write pass in the same order
-        // each warp a contiguous block of pairs (whole multiples of 32)
-        const int lane = tid & 31, wid = tid >> 5;
-        const uint32_t blk = ((nPairs + NWARP * 32 - 1) / (NWARP * 32)) * 32;
-        const uint32_t gw = (uint32_t)wid * blk, ge = min(nPairs, gw + blk);
-        uint32_t mine = lane_pairs<false>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0,
-                                          item, 0, false);
-        uint32_t off, d1, d2, tot[3];
-        block_scan3(mine, 0u, 0u, off, d1, d2, tot, ts.wsum);
-        if (tid == 0) {
-            ts.cnt[K_SETS4] += tot[0];
-            s_base = 0;
-            s_store = 0;
-            if (!noext && tot[0]) {
-                s_base = atomicAdd(&a.status->n_jobs, (ull)tot[0]);
-                if (s_base + tot[0] <= a.jobs_cap) s_store = 1;
-                else raise_capacity(a.status, E_QUEUE, 5, s_base + tot[0], a.jobs_cap, S0);
+        const uint64_t c0 = s_claim;
+        const bool stop = c0 >= a.n_tiles || ts.skip;
+        __syncthreads();                                                 // s_claim read by all
+        if (stop) break;                                                 // block-uniform
+        const uint64_t cn = min((uint64_t)SUPER_K, a.n_tiles - c0);
+        uint64_t ti = a.n_tiles - c0 - cn;
+        const uint64_t ti_end = a.n_tiles - c0;
+        while (ti < ti_end) {
+            // a group: the claimed tiles of one segment, one scan for all of them
+            uint32_t lo = 0, hi = a.n_items;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.items[mid].tile_base <= ti) lo = mid; else hi = mid;
             }
+            const Item it = a.items[lo];
+            const uint64_t seg_tiles = (it.hi - it.lo + (1ull << TL) - 1) >> TL;
+            const uint64_t g_end = min(ti_end, it.tile_base + seg_tiles);
+            const uint32_t ng = (uint32_t)(g_end - ti);
+            const uint64_t SA = it.lo + ((ti - it.tile_base) << TL);
+            const uint64_t SB = min(it.hi, SA + ((uint64_t)ng << TL));
+            const uint32_t item = it.id;
+            const bool grouped = lists != nullptr && SA >= SUPER_MIN_S;
+            if (grouped) {
+                if (tid < SUPER_K * NWARP) raw_n[tid] = 0;
+                __syncthreads();
+                scan_group(SA, SB, TL, lists, a.raw_cap, raw_n, slice);
+                __syncthreads();
+            }
+            for (uint32_t j = 0; j < ng; j++) {
+                tile_reset(ts);
+                __syncthreads();
+                const uint64_t S0 = SA + ((uint64_t)j << TL);
+                const uint32_t n = (uint32_t)min((uint64_t)L::W, SB - S0);
+                bool use_list = grouped;
+                for (int w = 0; w < NWARP; w++) use_list = use_list && raw_n[j * NWARP + w] <= slice;
+                if (!tile_reps<TL>(a, ts, smem, S0, n, use_list ? lists + (size_t)j * a.raw_cap : nullptr,
+                                   &raw_n[j * NWARP], slice)) { __syncthreads(); continue; }
+                const uint16_t *is_off = (const uint16_t *)(smem + L::OFF_IS_OFF);
+                const uint16_t *is_k = (const uint16_t *)(smem + L::OFF_IS_K);
+                const uint16_t *is_start = (const uint16_t *)(smem + L::OFF_IS_START);
+                const uint32_t *is_pbase = (const uint32_t *)(smem + L::OFF_IS_PBASE);
+                const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
+                const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
+                const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
+                // count pass, one reservation for the tile, write pass in the same order
+                // each warp a contiguous block of pairs (whole multiples of 32)
+                const int lane = tid & 31, wid = tid >> 5;
+                const uint32_t blk = ((nPairs + NWARP * 32 - 1) / (NWARP * 32)) * 32;
+                const uint32_t gw = (uint32_t)wid * blk, ge = min(nPairs, gw + blk);
+                uint32_t mine = lane_pairs<false>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0,
+                                                  item, 0, false);
+                uint32_t off, d1, d2, tot[3];
+                block_scan3(mine, 0u, 0u, off, d1, d2, tot, ts.wsum);
+                if (tid == 0) {
+                    ts.cnt[K_SETS4] += tot[0];
+                    s_base = 0;
+                    s_store = 0;
+                    if (!noext && tot[0]) {
+                        s_base = atomicAdd(&a.status->n_jobs, (ull)tot[0]);
+                        if (s_base + tot[0] <= a.jobs_cap) s_store = 1;
+                        else raise_capacity(a.status, E_QUEUE, 5, s_base + tot[0], a.jobs_cap, S0);
+                    }
+                }
+                __syncthreads();
+                if (need_write_pass) {
+                    const bool store = s_store != 0;
+                    lane_pairs<true>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item,
+                                     s_base + off, store);
+                }
+                __syncthreads();
+                tile_flush_counters(a, ts, item);
+                __syncthreads();
+            }
+            ti = g_end;
         }
-        __syncthreads();
-        if (need_write_pass) {
-            const bool store = s_store != 0;
-            lane_pairs<true>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item,
-                             s_base + off, store);
-        }
-        __syncthreads();
-        tile_flush_counters(a, ts, item);
-        __syncthreads();
     }
 }
 
@@ -738,7 +779,8 @@ int ext_grid(int num_sms) { return num_sms * 3; }
 
 template <int TL>
 static int launch_gen_tl(const SearchArgs &a, int grid, cudaStream_t s) {
-    const size_t smem = TileLayout<TL>::BYTES;
+    // the tile layout up to its extension-list area, then the group's list counters there
+    const size_t smem = TileLayout<TL>::OFF_ELIST + SUPER_K * NWARP * sizeof(uint32_t);
     cudaFuncSetAttribute(gen_jobs<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     gen_jobs<TL><<<grid, BS, smem, s>>>(a);
     return (int)cudaGetLastError();

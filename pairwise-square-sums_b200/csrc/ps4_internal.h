@@ -74,14 +74,17 @@ struct SearchArgs {
     uint32_t flags;            // PS4_F_*
     uint32_t *jobs;            // 4-set job queue between gen_jobs and extend_jobs: 6 * jobs_cap u32 (SoA)
     uint64_t jobs_cap;
-    uint64_t *raw;             // optional (gen_jobs): per-CTA list of every representation of the tile,
-    uint32_t raw_cap;          //   raw_cap entries per CTA in NWARP equal warp slices
+    uint64_t *raw;             // optional (gen_jobs): per CTA, SUPER_K lists of one tile's representations,
+    uint32_t raw_cap;          //   raw_cap entries each, in NWARP equal warp slices
 };
-// representations a tile's raw list holds per CTA: (pi/8) * 2^14 = 6434 expected, 8192 with margin
-constexpr uint32_t RAW_PER_CTA = 8192;
-// the raw list pays from S ~ 1e10 up (measured on B200: 1.25x faster tile kernel at 1e11, break-even
-// at 1e10, slower below): the fill pass's rescan costs ~sqrt(S) steps per tile, recording ~W/3
-constexpr uint64_t RAW_MIN_S = 10000000000ull;
+// representations a tile's list holds: (pi/8) * 2^14 = 6434 expected, 8192 with margin
+constexpr uint32_t RAW_PER_TILE = 8192;
+// tiles a tile-kernel CTA claims at once and scans as one range: the scan of a tile costs
+// ~0.29 sqrt(S) steps whatever its width, so one scan of SUPER_K adjacent tiles, recorded into
+// their lists, divides that cost by SUPER_K (lists: 296 CTAs x 8 x 64 KB = 155 MB)
+constexpr uint32_t SUPER_K = 8;
+// below this S a tile's own scan is cheaper than recording and reading the lists
+constexpr uint64_t SUPER_MIN_S = 10000000000ull;
 
 // Arguments of one triple-extension launch (ps4_triples.cu).
 struct TriArgs {

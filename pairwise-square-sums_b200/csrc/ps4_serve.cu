@@ -592,7 +592,7 @@ int launch_step(ps4_server *s, StepBuf &b) {
         a.flags = s->v.flags & ~(uint32_t)PS4_F_DUMP4;
         a.jobs = s->d_jobs; a.jobs_cap = s->jobs_cap;
         if (!b.fused) {
-            a.raw = s->d_raw; a.raw_cap = RAW_PER_CTA;
+            a.raw = s->d_raw; a.raw_cap = RAW_PER_TILE;
             const int g = (int)std::min<uint64_t>((uint64_t)gen_grid(s->v.num_sms), std::max<uint64_t>(tiles, 1));
             SRV_CUDA(s, (cudaError_t)launch_gen(a, g, st));
             if (!(s->v.flags & PS4_F_NOEXT)) SRV_CUDA(s, (cudaError_t)launch_ext(a, ext_grid(s->v.num_sms), st));
@@ -939,7 +939,7 @@ extern "C" int ps4_serve_create(ps4_ctx *ctx, const ps4_serve_config *cfg, ps4_s
     s->jobs_cap = 1ull << 20;
     while (s->jobs_cap < (1ull << 27) && (double)s->jobs_cap < need) s->jobs_cap <<= 1;
     if (dev_alloc(s, s->d_jobs, 6 * s->jobs_cap)) return PS4_ERR_CUDA;
-    if (dev_alloc(s, s->d_raw, (uint64_t)gen_grid(s->v.num_sms) * RAW_PER_CTA)) return PS4_ERR_CUDA;
+    if (dev_alloc(s, s->d_raw, (uint64_t)gen_grid(s->v.num_sms) * SUPER_K * RAW_PER_TILE)) return PS4_ERR_CUDA;
     if (dev_alloc(s, s->d_slots, c.max_slots)) return PS4_ERR_CUDA;
     for (int i = 0; i < 2; i++)
         if (init_buf(s, s->buf[i])) return PS4_ERR_CUDA;
