@@ -324,6 +324,15 @@ def read_traffic_per_S(kernel: str):
     return float(m.group(1)) if m else None
 
 
+def read_issue_active(kernel: str):
+    """Fraction of issue slots busy (smsp__issue_active) of one kernel, from its ncu summary."""
+    p = REPO / "profiles" / f"ncu_{kernel}_5e9.txt"
+    if not p.exists():
+        return None
+    m = re.search(r"issue slots busy \(smsp__issue_active\)\s+([\d.]+) %", p.read_text())
+    return float(m.group(1)) / 100 if m else None
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -490,8 +499,9 @@ def main():
                         "achieved": ops_ext / (ext_ms / 1e3) if ext_ms else None,
                         "traffic_per_step": (read_traffic_per_S("extend_jobs") or 0) * (hi - lo) or None},
     }
-    for k in kernels.values():
+    for name, k in kernels.items():
         k["frac"] = k["achieved"] / peak if k["achieved"] else None
+        k["issue_active_ncu"] = read_issue_active(name)
     dom = "extend_jobs" if ext_ms >= gen_ms else "gen_jobs"
     line = {
         "metric": METRIC, "value": S_all / dev_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -511,6 +521,8 @@ def main():
                      "per": "step (all launches of the kernel in one search of the range; a step is "
                             f"{launches // max(args.steps, 1) // 2} batches)",
                      "ops": kernels[dom]["ops_per_step"], "traffic": kernels[dom]["traffic_per_step"],
+                     "issue_active_ncu": kernels[dom]["issue_active_ncu"],
+                     "issue_active_source": f"profiles/ncu_{dom}_5e9.txt (1e8-S capture at S = 5e9)",
                      "step_achieved": achieved_step, "step_frac": achieved_step / peak,
                      "kernels": kernels},
         "e2e": {"value": S_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
