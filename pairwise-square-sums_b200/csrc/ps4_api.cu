@@ -552,7 +552,7 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
             return set_err(c, PS4_ERR_CUDA, "job queue overflow persists near S=%llu", errS);
         }
         if (code == E_EXTLIST && c->cfg.kernel == PS4_KERNEL_BATCHED && !c->fused_fallback) {
-            c->fused_fallback = true;            // > 16 extensions in one engine warp batch: fused kernel
+            c->fused_fallback = true;            // more extensions in one engine round than its list holds: fused kernel
             continue;
         }
         if (code == E_TILE || code == E_EXTLIST) {

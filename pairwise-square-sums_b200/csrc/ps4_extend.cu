@@ -226,7 +226,7 @@ constexpr int EBS = 256;                 // threads per CTA
 constexpr int EWARPS = EBS / 32;
 constexpr int DCAP = 416;                // divisor-list entries per warp (u64)
 constexpr int QCAP = 64;                 // square-test queue per warp
-constexpr int EXCAP = 8;                 // extensions per warp batch
+constexpr int EXCAP = 8;                 // extensions per warp and round
 constexpr int FSLOT = 16;                // prime slots per lane: m1's primes from 0, m2's from 8
 
 // The odd part D_odd of a difference is kept factored: its odd primes are split into a low
@@ -324,7 +324,7 @@ struct LaneCounters {
     }
 };
 
-// Report the extensions of one warp batch: group them per 4-set, emit hit / ext / six
+// Report the extensions of one warp round: group them per 4-set, emit hit / ext / six
 // records and the counters sets5 / multi / sets6 / hist5 / max_extensions (s4.c:243-277).
 static __device__ void report_warp_exts(const SearchArgs &a, ExtEntry *el, uint32_t n) {
     for (uint32_t x = 1; x < n; x++) {

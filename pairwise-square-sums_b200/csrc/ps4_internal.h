@@ -27,7 +27,7 @@ enum {
     E_CAP_EXT = PS4_ERR_CAP_EXT,
     E_VERIFY = PS4_ERR_VERIFY,
     E_TILE = 100,      // a tile outgrew its shared-memory lists: re-run with smaller tiles
-    E_EXTLIST = 101,   // more extensions in one tile than the per-tile list holds: re-run smaller
+    E_EXTLIST = 101,   // more extensions than a tile's (fused kernel) or an engine round's list holds
     E_QUEUE = 102      // the 4-set job queue of a batch overflowed: re-run with narrower batches
 };
 
@@ -49,8 +49,8 @@ struct Status {
     unsigned long long diag[4];    // first internal-capacity event: which list, size, limit, S
     // per batch of the two-kernel pipeline (cleared before every batch)
     unsigned long long n_jobs;     // 4-sets queued by gen_jobs
-    unsigned int tile_next;        // tile work counter of the tile kernels
-    unsigned int ext_next;         // extend_jobs work counter (warp batches handed out)
+    unsigned int tile_next;        // tile work counter of the tile kernels (tiles handed out)
+    unsigned int ext_next;         // extend_jobs work counter (queued 4-sets handed out)
 };
 
 // Arguments of one search launch (passed by value).
