@@ -125,6 +125,21 @@ def test_frontier_blocks(golden, big):
         assert_stats_equal(r.stats, blk, hist=False, label=blk["block"])
 
 
+def test_frontier_blocks_wide():
+    """Eight more archived blocks spread over S ~ 2.15e12 .. 3.51e12 (exhaustive-2026-09-18 and
+    -09-19 raw evidence; tests/golden/make_frontier.py), where the tile kernel scans groups of
+    tiles into per-tile lists: sorted-output hash, every M line, every TOTAL counter."""
+    import json
+    blocks = json.loads((GOLDEN_DIR / "frontier.json").read_text())
+    with Search(max(b["hi"] for b in blocks) + 1) as s:
+        for blk in blocks:
+            r = s.range(blk["lo"], blk["hi"])
+            assert sha_sorted(r.lines) == blk["sha256"], blk["block"]
+            assert len(r.lines) == blk["n_lines"]
+            assert sorted(x for x in r.lines if x.startswith("M:")) == blk["m_lines"], blk["block"]
+            assert_stats_equal(r.stats, blk, hist=False, label=blk["block"])
+
+
 @pytest.mark.parametrize("seed", range(8))
 def test_fresh_ranges_against_oracle(big, seed):
     rng = random.Random(77 + seed)
