@@ -13,8 +13,15 @@
  * searched on the GPU one batch of whole chunks at a time.  Capacity caps can be lowered
  * for failure-injection tests through the environment variables S4_MAX_REPS / S4_MAX_DIVS /
  * S4_MAX_EXT (the reference's compile-time macros of the same names, s4.c:45-54).
+ *
+ * SIGTERM / SIGINT (a block controller's deadline, run_exhaustive.py:221-224) stop the run at
+ * the next batch boundary: the checkpoint is written with the positions reached (no DONE),
+ * the results are flushed, and the signal is raised again with its default action, so the
+ * exit status is the reference's (killed by that signal) and a --resume continues without
+ * repeating or losing a line.  No kernel is cut off mid-launch.
  */
 #define _GNU_SOURCE
+#include <signal.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -265,6 +272,9 @@ static void run_batch(ps4_ctx *ctx, region_t *rg, u64 lo, u64 hi, batch_out *b) 
     write_out(b->text, b->text_len);
 }
 
+static volatile sig_atomic_t stop_signal = 0;
+static void on_stop_signal(int sig) { stop_signal = sig; }
+
 static unsigned env_cap(const char *name, unsigned dflt) {
     const char *s = getenv(name);
     return s && *s ? (unsigned)strtoul(s, NULL, 10) : dflt;
@@ -318,6 +328,13 @@ int main(int argc, char **argv) {
                 (unsigned long long)S_lo, (unsigned long long)S_hi);
         return 0;
     }
+    struct sigaction sa;
+    memset(&sa, 0, sizeof sa);
+    sa.sa_handler = on_stop_signal;
+    sigemptyset(&sa.sa_mask);
+    sa.sa_flags = SA_RESTART;
+    sigaction(SIGTERM, &sa, NULL);
+    sigaction(SIGINT, &sa, NULL);
     ps4_config cfg;
     memset(&cfg, 0, sizeof cfg);
     cfg.device = 0;
@@ -348,9 +365,9 @@ int main(int argc, char **argv) {
     double t0 = now_sec(), last_ckpt = -1e9;
     int last_report = 0;
     u64 chunks_per_batch = 1;
-    for (int t = 0; t < nthreads; t++) {
+    for (int t = 0; t < nthreads && !stop_signal; t++) {
         double rt0 = now_sec();
-        for (u64 S0 = rg[t].region_lo; S0 < rg[t].region_hi;) {
+        for (u64 S0 = rg[t].region_lo; S0 < rg[t].region_hi && !stop_signal;) {
             u64 span = chunks_per_batch * W;
             u64 S1 = rg[t].region_hi - S0 > span ? S0 + span : rg[t].region_hi;
             double b0 = now_sec();
@@ -375,6 +392,18 @@ int main(int argc, char **argv) {
             }
         }
         rg[t].secs = now_sec() - rt0;
+    }
+    if (stop_signal) {
+        const int sig = stop_signal;
+        write_ckpt(rg, 0);
+        fprintf(stderr, "s4gpu: stopped by signal %d at a batch boundary%s\n", sig,
+                opt_ckpt ? "; the checkpoint holds the positions reached" : "");
+        fflush(stderr);
+        ps4_destroy(ctx);
+        if (out_fp != stdout) fclose(out_fp); else fflush(stdout);
+        signal(sig, SIG_DFL);
+        raise(sig);
+        return 128 + sig;
     }
     double el = now_sec() - t0;
     write_ckpt(rg, 1);

@@ -1,14 +1,19 @@
 """The drop-in CLI (bin/s4gpu) on the GPU, checked the way the reference's own preflight
 test checks s4 (archived test_preflight.py): small census equality as sorted line lists,
 injected capacity failures with exit 2, and kill/resume equivalence; plus the stderr and
-checkpoint formats its consumers parse (verify.py:102-136, compact.py:29-45)."""
+checkpoint formats its consumers parse (verify.py:102-136, compact.py:29-45), consecutive blocks
+driven as the archived block controller drives s4 (run_exhaustive.py:200-248), and the stop on
+the controller's SIGTERM with its resume."""
 from __future__ import annotations
 
 import re
+import signal
 import subprocess
+import time
 
 import pytest
 
+import consumers
 from conftest import PKG, assert_stats_equal, sha_sorted
 from golden.make_golden import parse_stderr
 from oracle import orc
@@ -113,3 +118,65 @@ def test_cli_matches_reference_order_single_region(tmp_path):
     run([10 ** 8, 10 ** 8 + 3 * 10 ** 6, 1, 18, "--out", "o.out"], tmp_path)
     _, _, olines, _ = orc.search(10 ** 8, 10 ** 8 + 3 * 10 ** 6)
     assert (tmp_path / "o.out").read_text() == "".join(olines)
+
+
+def test_cli_block_controller_contract(tmp_path):
+    """Three consecutive blocks from the controller's default frontier, each started, read back
+    and sized as the archived block controller does (run_exhaustive.py:200-248), then audited as
+    the packer and the verifier audit a block (compact.py:29-45, verify.py:140-164)."""
+    frontier, done = 1_001_000_000_000, []
+    for k in range(3):
+        width = consumers.next_width(done, available_s=6.0)
+        assert width >= 10 ** 8
+        name = "block-%04d" % (k + 1)
+        lo, hi = frontier, frontier + width
+        rc, secs = consumers.run_block(CLI, tmp_path, name, lo, hi)
+        assert rc == 0, (tmp_path / (name + ".err")).read_text()
+        err = (tmp_path / (name + ".err")).read_text()
+        ckpt = (tmp_path / (name + ".ckpt")).read_text()
+        totals, maxima = consumers.parse_block(err, ckpt, lo, hi)
+        consumers.check_checkpoint(ckpt, lo, hi, 16, 20, totals)
+        lines = (tmp_path / (name + ".out")).read_text().splitlines(keepends=True)
+        counts, five, near, max_ext = consumers.scan(lines, lo, hi)
+        assert counts["multi"] == totals["multi-ext-4sets"] and totals["6-sets"] == 0
+        assert max_ext <= maxima["extensions"][0]
+        done.append({"lo": lo, "hi": hi, "elapsed": secs})
+        frontier = hi
+    assert not (tmp_path / "SIXSET_FOUND.txt").exists()
+    assert [b["lo"] for b in done[1:]] == [b["hi"] for b in done[:-1]]       # contiguous frontier
+
+
+def test_cli_sigterm_stops_at_a_batch_and_resumes(tmp_path):
+    """The controller's deadline (run_exhaustive.py:221-224: SIGTERM, SIGKILL 10 s later): the
+    CLI stops at the next batch boundary with the reference's exit status (killed by SIGTERM),
+    prints no TOTAL line, leaves a checkpoint of the positions reached, and --resume completes
+    the interval with the counters and result lines, none repeated, of one uninterrupted run."""
+    lo, hi, T = 10 ** 11, 10 ** 11 + 3 * 10 ** 10, 16
+    whole, part = tmp_path / "whole", tmp_path / "part"
+    whole.mkdir()
+    part.mkdir()
+    ref = run([lo, hi, T, 20, "--out", "w.out", "--ckpt", "w.ckpt"], whole)
+    args = [str(CLI), str(lo), str(hi), str(T), "20", "--out", "p.out", "--ckpt", "p.ckpt"]
+    with (part / "p.err").open("w") as log:
+        p = subprocess.Popen(args, cwd=part, stdout=subprocess.DEVNULL, stderr=log)
+        t0 = time.monotonic()
+        while not (part / "p.ckpt").exists() and p.poll() is None and time.monotonic() - t0 < 120:
+            time.sleep(0.005)               # the first checkpoint follows the first batch
+        p.send_signal(signal.SIGTERM)
+        rc = p.wait(timeout=60)
+    err = (part / "p.err").read_text()
+    assert rc == -signal.SIGTERM, err
+    assert "TOTAL:" not in err and "stopped by signal 15" in err
+    ck = (part / "p.ckpt").read_text().splitlines()
+    assert ck[0] == "s4ckpt v1" and ck[-1] != "DONE" and len(ck) == T + 2
+    rows = [list(map(int, x.split())) for x in ck[2:]]
+    assert any(r[1] < r[2] for r in rows)                                    # stopped part-way
+    assert all(r[3] == r[1] - (lo + (hi - lo) * r[0] // T) for r in rows)    # S_done = positions reached
+    res = run([lo, hi, T, 20, "--out", "p.out", "--ckpt", "p.ckpt", "--resume"], part)
+    assert "RESUMED from checkpoint" in res.stderr
+    assert (part / "p.ckpt").read_text().endswith("DONE\n")
+    assert_stats_equal(parse_stderr(res.stderr), parse_stderr(ref.stderr), hist=False, maxima=False,
+                       label="stopped + resumed")
+    got = (part / "p.out").read_text().splitlines()
+    want = (whole / "w.out").read_text().splitlines()
+    assert len(got) == len(set(got)) and sorted(got) == sorted(want)
