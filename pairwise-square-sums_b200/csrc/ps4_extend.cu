@@ -237,11 +237,12 @@ constexpr int FSLOT = 16;                // prime slots per lane: m1's primes fr
 struct __align__(16) EJob {              // one lane's 4-set, read by every lane in phase B
     uint64_t m64, m63, m65;              // bit s: u^2 + (C - A) is a residue for both C (mod 64/63/65)
     uint64_t A;                          // extend by D = A - B
-    uint32_t uA, uS;                     // u <= uA: e <= 0;  u <= uS: e <= max(v)
-    uint32_t ncand, item;
+    uint32_t uA, rAA;                    // u <= uA: e <= 0;  rAA = sqrt(2A) if integral, else 0
+    uint32_t ncand, rAB;                 // rAB = sqrt(A + B)
     uint16_t base, L, H;                 // lo list at dbuf[base..base+L), hi list right after it
     uint8_t E2, flags;                   // flags: 1 = D even, 2 = residue 64 passes mod 65
-    uint64_t B;                          // the smaller member of the difference (e in v check)
+    uint32_t rAC1, rAC2;                 // sqrt(A + C1), sqrt(A + C2): e = u^2 - A is a member of
+                                         //   the 4-set iff u is one of rAA, rAB, rAC1, rAC2
     uint64_t C1, C2;                     // the other two members (square tests)
 };
 
@@ -414,7 +415,7 @@ static __device__ void report_warp_exts(const SearchArgs &a, ExtEntry *el, uint3
 struct LaneJob {
     uint32_t r[6], item;
     uint64_t v[4], S, A, C1, C2;
-    int bi, bj, bk;
+    int bi, bj, bk, o1, o2;              // A = v[bi], B = v[bj], C1 = v[o1], C2 = v[o2]
     int np;                              // distinct primes, in w->fp[0..np)[lane]
     bool has2;
     int E2, j0, js;                      // odd primes are pr[j0..np); the high group starts at js
@@ -477,6 +478,8 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
         if (t != J.bi && t != J.bj) { if (o1 < 0) o1 = t; else o2 = t; }
     J.C1 = pick4(J.v, o1);
     J.C2 = pick4(J.v, o2);
+    J.o1 = o1;
+    J.o2 = o2;
     J.np = factor_pair(a.spfq, ra - rb, ra + rb, fp, lane);
     // D even => both factors even => 2 is the first prime and 4 | D
     J.has2 = J.np > 0 && (fp[0][lane] & 0xFFFFFFu) == 2;
@@ -634,11 +637,14 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 E.m63 = UQ.q63[a63] & UQ.q63[b63];
                 E.m65 = UQ.q65[a65] & UQ.q65[b65];
                 const uint32_t h1 = UQ.q65top[a65], h2 = UQ.q65top[b65];
-                uint64_t vmax = J.v[0];
-                for (int i = 1; i < 4; i++) vmax = J.v[i] > vmax ? J.v[i] : vmax;
                 E.uA = isqrt_lt2p46(J.A);                        // < 2^22 (A < 2^44)
-                E.uS = isqrt_lt2p46(J.A + vmax);                 // < 2^23
-                E.B = pick4(J.v, J.bj); E.ncand = J.ncand; E.item = J.item;
+                const uint32_t r2A = isqrt_lt2p46(2 * J.A);      // < 2^23
+                E.rAA = (uint64_t)r2A * r2A == 2 * J.A ? r2A : 0u;
+                // the 4-set's own roots: r[pair_slot(i, j)]^2 = v_i + v_j
+                E.rAB = pick6(J.r, pair_slot(J.bi, J.bj));
+                E.rAC1 = pick6(J.r, pair_slot(J.bi, J.o1));
+                E.rAC2 = pick6(J.r, pair_slot(J.bi, J.o2));
+                E.ncand = J.ncand;
                 E.base = (uint16_t)base; E.L = (uint16_t)J.L; E.H = (uint16_t)J.H;
                 E.E2 = (uint8_t)J.E2;
                 E.flags = (uint8_t)((J.has2 ? 1 : 0) | ((h1 & h2) << 1));
@@ -669,7 +675,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             }
             // the current job of this lane's run, in registers
             uint64_t A = 0, m64 = 0, m63 = 0, m65 = 0, hv = 0, hc = 0;
-            uint32_t uA = 0, uS = 0;
+            uint32_t uA = 0, rAA = 0, rAB = 0, rAC1 = 0, rAC2 = 0;
             uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1, dlo = 0, dhi = 0;
             uint32_t cc = 0, l = 0, h = 0, d2 = 0;
             // job fields in four vector loads; entering a job at its first candidate needs no division
@@ -678,8 +684,10 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 const ulonglong2 x0 = E2p[0], x1 = E2p[1];
                 const uint4 y = *(const uint4 *)&w->job[j].uA;
                 const uint2 z = *(const uint2 *)&w->job[j].base;
+                const uint2 rr2 = *(const uint2 *)&w->job[j].rAC1;
                 m64 = x0.x; m63 = x0.y; m65 = x1.x; A = x1.y;
-                uA = y.x; uS = y.y; ncand = y.z;
+                uA = y.x; rAA = y.y; ncand = y.z; rAB = y.w;
+                rAC1 = rr2.x; rAC2 = rr2.y;
                 jb = z.x & 0xFFFFu; L = z.x >> 16; H = z.y & 0xFFFFu; E2 = (z.y >> 16) & 0xFFu; flg = z.y >> 24;
                 R = (flg & 1) ? E2 - 1 : 1;
                 dlo = flg & 1; dhi = (flg & 1) ? E2 - 1 : 0;      // 2-exponents of f: [1, E2-1] or {0}
@@ -711,12 +719,11 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     const uint32_t rr = (uint32_t)(u >> 24) + ((uint32_t)u & 0xFFFFFFu);   // 2^24 = 1 mod 63, 65
                     const uint32_t w63 = rr % 63u, w65 = rr % 65u;
                     const uint32_t b65 = w65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65 >> w65) & 1u;
-                    pass = (((m64 >> w64) & (m63 >> w63) & 1u) & b65) && u > uA;
-                    if (pass && u <= uS) {                  // e <= max(v): rule out e in v (s4.c:197)
-                        const uint64_t e = u * u - A;       // u < 2^23
-                        const EJob &Ej = w->job[jcur];
-                        if (e == A || e == Ej.B || e == Ej.C1 || e == Ej.C2) pass = false;
-                    }
+                    // e = u^2 - A in v (s4.c:197) iff u^2 = A + v_i: u is one of the 4-set's roots
+                    // through A (all below 2^23, so u's low word decides once u < 2^32)
+                    const uint32_t ul = (uint32_t)u;
+                    const bool member = (u >> 32) == 0 && (ul == rAB || ul == rAC1 || ul == rAC2 || ul == rAA);
+                    pass = (((m64 >> w64) & (m63 >> w63) & 1u) & b65) && u > uA && !member;
                     if (pass) { sq_run++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
                     {                                          // (l, h, d2) advance, branch-free
