@@ -236,13 +236,13 @@ constexpr int FSLOT = 16;                // prime slots per lane: m1's primes fr
 // L+H entries instead of ndo = L*H.
 struct __align__(16) EJob {              // one lane's 4-set, read by every lane in phase B
     uint64_t m64, m63, m65;              // bit s: u^2 + (C - A) is a residue for both C (mod 64/63/65)
-    uint64_t A;                          // extend by D = A - B
-    uint32_t uA, rAA;                    // u <= uA: e <= 0;  rAA = sqrt(2A) if integral, else 0
-    uint32_t ncand, rAB;                 // rAB = sqrt(A + B)
+    uint32_t rAB, rAC1;                  // sqrt(A + B), sqrt(A + C1)
+    uint32_t uA, rAA, rAC2, ncand;       // u <= uA: e <= 0; rAA = sqrt(2A) if integral, else 0;
+                                         //   e = u^2 - A is a member of the 4-set iff u is one of
+                                         //   rAA, rAB, rAC1, rAC2
     uint16_t base, L, H;                 // lo list at dbuf[base..base+L), hi list right after it
-    uint8_t E2, flags;                   // flags: 1 = D even, 2 = residue 64 passes mod 65
-    uint32_t rAC1, rAC2;                 // sqrt(A + C1), sqrt(A + C2): e = u^2 - A is a member of
-                                         //   the 4-set iff u is one of rAA, rAB, rAC1, rAC2
+    uint8_t E2, flags;                   // flags: 1 = D even
+    uint64_t A;                          // extend by D = A - B
     uint64_t C1, C2;                     // the other two members (square tests)
 };
 
@@ -266,10 +266,10 @@ static_assert(EWARPS * sizeof(WarpArea) + 1024 <= 228 * 1024 / 3, "three engine 
 // Residue masks indexed by u's residue: bit w of q_m[a] is set iff w^2 + a is a square mod m.
 // A 4-set's mask for its two remaining members C1, C2 is q_m[(C1-A) mod m] & q_m[(C2-A) mod m],
 // so the filters of e + C = u^2 + (C - A) (s4.c:192-194) become one bit test per modulus on
-// u mod m.  Mod 65 needs 65 bits: bit 64 lives in q65top.
+// u mod m.  Mod 65 has 65 residues, but 64 = -1 and 1 have the same square, so bit 64 equals
+// bit 1 and residue 64 is looked up as 1.
 struct UResTabs {
     uint64_t q64[64], q63[63], q65[65];
-    uint8_t q65top[65];
 };
 constexpr bool is_qr_mod(int m, int r) {
     return r < 64 ? ((qr_bits(m) >> r) & 1) != 0 : true;          // r = 64 (m = 65) is 8^2
@@ -290,7 +290,6 @@ constexpr UResTabs make_ures() {
         uint64_t x = 0;
         for (int w = 0; w < 64; w++) if (is_qr_mod(65, (w * w + a) % 65)) x |= 1ull << w;
         t.q65[a] = x;
-        t.q65top[a] = is_qr_mod(65, (64 * 64 + a) % 65) ? 1 : 0;
     }
     return t;
 }
@@ -636,7 +635,6 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 E.m64 = UQ.q64[(uint32_t)dd1 & 63u] & UQ.q64[(uint32_t)dd2 & 63u];
                 E.m63 = UQ.q63[a63] & UQ.q63[b63];
                 E.m65 = UQ.q65[a65] & UQ.q65[b65];
-                const uint32_t h1 = UQ.q65top[a65], h2 = UQ.q65top[b65];
                 E.uA = isqrt_lt2p46(J.A);                        // < 2^22 (A < 2^44)
                 const uint32_t r2A = isqrt_lt2p46(2 * J.A);      // < 2^23
                 E.rAA = (uint64_t)r2A * r2A == 2 * J.A ? r2A : 0u;
@@ -647,7 +645,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 E.ncand = J.ncand;
                 E.base = (uint16_t)base; E.L = (uint16_t)J.L; E.H = (uint16_t)J.H;
                 E.E2 = (uint8_t)J.E2;
-                E.flags = (uint8_t)((J.has2 ? 1 : 0) | ((h1 & h2) << 1));
+                E.flags = (uint8_t)(J.has2 ? 1 : 0);
             }
             // ---- phase B: the pooled candidates, 32 equal contiguous runs
             const uint32_t nc = fits ? J.ncand : 0;
@@ -674,20 +672,19 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 jl = lo;
             }
             // the current job of this lane's run, in registers
-            uint64_t A = 0, m64 = 0, m63 = 0, m65 = 0, hv = 0, hc = 0;
+            uint64_t m64 = 0, m63 = 0, m65 = 0, hv = 0, hc = 0;
             uint32_t uA = 0, rAA = 0, rAB = 0, rAC1 = 0, rAC2 = 0;
             uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1, dlo = 0, dhi = 0;
             uint32_t cc = 0, l = 0, h = 0, d2 = 0;
             // job fields in four vector loads; entering a job at its first candidate needs no division
             auto load_job = [&](uint32_t j) {
-                const ulonglong2 *E2p = (const ulonglong2 *)&w->job[j];
-                const ulonglong2 x0 = E2p[0], x1 = E2p[1];
+                const ulonglong2 x0 = *(const ulonglong2 *)&w->job[j].m64;
+                const ulonglong2 x1 = *(const ulonglong2 *)&w->job[j].m65;    // m65, rAB | rAC1 << 32
                 const uint4 y = *(const uint4 *)&w->job[j].uA;
                 const uint2 z = *(const uint2 *)&w->job[j].base;
-                const uint2 rr2 = *(const uint2 *)&w->job[j].rAC1;
-                m64 = x0.x; m63 = x0.y; m65 = x1.x; A = x1.y;
-                uA = y.x; rAA = y.y; ncand = y.z; rAB = y.w;
-                rAC1 = rr2.x; rAC2 = rr2.y;
+                m64 = x0.x; m63 = x0.y; m65 = x1.x;
+                rAB = (uint32_t)x1.y; rAC1 = (uint32_t)(x1.y >> 32);
+                uA = y.x; rAA = y.y; rAC2 = y.z; ncand = y.w;
                 jb = z.x & 0xFFFFu; L = z.x >> 16; H = z.y & 0xFFFFu; E2 = (z.y >> 16) & 0xFFu; flg = z.y >> 24;
                 R = (flg & 1) ? E2 - 1 : 1;
                 dlo = flg & 1; dhi = (flg & 1) ? E2 - 1 : 0;      // 2-exponents of f: [1, E2-1] or {0}
@@ -717,13 +714,13 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     // bits of the 4-set's u-indexed masks
                     const uint32_t w64 = (uint32_t)u & 63u;
                     const uint32_t rr = (uint32_t)(u >> 24) + ((uint32_t)u & 0xFFFFFFu);   // 2^24 = 1 mod 63, 65
-                    const uint32_t w63 = rr % 63u, w65 = rr % 65u;
-                    const uint32_t b65 = w65 == 64u ? (flg >> 1) & 1u : (uint32_t)(m65 >> w65) & 1u;
+                    const uint32_t w63 = rr % 63u, w65r = rr % 65u;
+                    const uint32_t w65 = w65r == 64u ? 1u : w65r;     // 64^2 = 1^2 mod 65: same bit
                     // e = u^2 - A in v (s4.c:197) iff u^2 = A + v_i: u is one of the 4-set's roots
                     // through A (all below 2^23, so u's low word decides once u < 2^32)
                     const uint32_t ul = (uint32_t)u;
                     const bool member = (u >> 32) == 0 && (ul == rAB || ul == rAC1 || ul == rAC2 || ul == rAA);
-                    pass = (((m64 >> w64) & (m63 >> w63) & 1u) & b65) && u > uA && !member;
+                    pass = ((m64 >> w64) & (m63 >> w63) & (m65 >> w65) & 1u) && u > uA && !member;
                     if (pass) { sq_run++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
                     {                                          // (l, h, d2) advance, branch-free
