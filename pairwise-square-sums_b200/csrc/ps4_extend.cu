@@ -502,18 +502,24 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
     return true;
 }
 
-// divisors of prod pr[q]^ex[q], q in [q0, q1), in mixed-radix order (first prime fastest)
+// The n divisors of prod pr[q]^ex[q], q in [q0, q1), in mixed-radix order (first prime
+// fastest), in one flat loop: prime q's block repeats the list so far ex[q] times, each copy
+// times p_q, so d[j] = d[j - cur] * p_q with cur the list length before q.
 __device__ __forceinline__ void gen_list(uint64_t *d, const uint32_t (*fp)[32], int lane,
-                                         int q0, int q1) {
+                                         int q0, uint32_t n) {
     d[0] = 1;
-    uint32_t nn = 1;
-    for (int q = q0; q < q1; q++) {
-        const uint32_t cur = nn, pq = fp[q][lane] & 0xFFFFFFu, eq = fp[q][lane] >> 24;
-        uint64_t pk = 1;
-        for (uint32_t e = 1; e <= eq; e++) {
-            pk *= pq;
-            for (uint32_t i = 0; i < cur; i++) d[nn++] = d[i] * pk;
+    if (n <= 1) return;
+    int q = q0;
+    uint32_t x = fp[q][lane];
+    uint32_t p = x & 0xFFFFFFu, cur = 1, end = (x >> 24) + 1;
+    for (uint32_t j = 1; j < n; j++) {
+        if (j == end) {
+            cur = end;
+            x = fp[++q][lane];
+            p = x & 0xFFFFFFu;
+            end = cur * ((x >> 24) + 1);
         }
+        d[j] = d[j - cur] * p;
     }
 }
 
@@ -624,8 +630,8 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             const bool fits = pending && incl <= (uint32_t)DCAP;
             if (fits) w->jid[lane] = myjob;
             if (fits) {
-                gen_list(w->dbuf + base, w->fp, lane, J.j0, J.js);              // lo: L entries
-                gen_list(w->dbuf + base + J.L, w->fp, lane, J.js, J.np);        // hi: H entries
+                gen_list(w->dbuf + base, w->fp, lane, J.j0, J.L);               // lo: L entries
+                gen_list(w->dbuf + base + J.L, w->fp, lane, J.js, J.H);         // hi: H entries
                 EJob &E = w->job[lane];
                 E.A = J.A; E.C1 = J.C1; E.C2 = J.C2;
                 const int64_t dd1 = (int64_t)J.C1 - (int64_t)J.A, dd2 = (int64_t)J.C2 - (int64_t)J.A;
