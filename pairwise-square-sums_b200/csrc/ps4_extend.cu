@@ -236,10 +236,10 @@ constexpr int FSLOT = 16;                // prime slots per lane: m1's primes fr
 // L+H entries instead of ndo = L*H.
 struct __align__(16) EJob {              // one lane's 4-set, read by every lane in phase B
     uint64_t m64, m63, m65;              // bit s: u^2 + (C - A) is a residue for both C (mod 64/63/65)
-    uint32_t rAB, rAC1;                  // sqrt(A + B), sqrt(A + C1)
-    uint32_t uA, rAA, rAC2, ncand;       // u <= uA: e <= 0; rAA = sqrt(2A) if integral, else 0;
+    uint32_t rA0, rA1;                   // rA0..rA2: the roots sqrt(A + v) of the three other members
+    uint32_t uA, rAA, rA2, ncand;        // u <= uA: e <= 0; rAA = sqrt(2A) if integral, else 0;
                                          //   e = u^2 - A is a member of the 4-set iff u is one of
-                                         //   rAA, rAB, rAC1, rAC2
+                                         //   rAA, rA0, rA1, rA2
     uint16_t base, L, H;                 // lo list at dbuf[base..base+L), hi list right after it
     uint8_t E2, flags;                   // flags: 1 = D even
     uint64_t A;                          // extend by D = A - B
@@ -414,7 +414,7 @@ static __device__ void report_warp_exts(const SearchArgs &a, ExtEntry *el, uint3
 struct LaneJob {
     uint32_t r[6], item;
     uint64_t v[4], S, A, C1, C2;
-    int bi, bj, bk, o1, o2;              // A = v[bi], B = v[bj], C1 = v[o1], C2 = v[o2]
+    int bi, bj, bk;
     int np;                              // distinct primes, in w->fp[0..np)[lane]
     bool has2;
     int E2, j0, js;                      // odd primes are pr[j0..np); the high group starts at js
@@ -477,8 +477,6 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
         if (t != J.bi && t != J.bj) { if (o1 < 0) o1 = t; else o2 = t; }
     J.C1 = pick4(J.v, o1);
     J.C2 = pick4(J.v, o2);
-    J.o1 = o1;
-    J.o2 = o2;
     J.np = factor_pair(a.spfq, ra - rb, ra + rb, fp, lane);
     // D even => both factors even => 2 is the first prime and 4 | D
     J.has2 = J.np > 0 && (fp[0][lane] & 0xFFFFFFu) == 2;
@@ -644,10 +642,13 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 E.uA = isqrt_lt2p46(J.A);                        // < 2^22 (A < 2^44)
                 const uint32_t r2A = isqrt_lt2p46(2 * J.A);      // < 2^23
                 E.rAA = (uint64_t)r2A * r2A == 2 * J.A ? r2A : 0u;
-                // the 4-set's own roots: r[pair_slot(i, j)]^2 = v_i + v_j
-                E.rAB = pick6(J.r, pair_slot(J.bi, J.bj));
-                E.rAC1 = pick6(J.r, pair_slot(J.bi, J.o1));
-                E.rAC2 = pick6(J.r, pair_slot(J.bi, J.o2));
+                // the three roots through A, r[pair_slot(bi, x)]^2 = A + v_x (the member test takes
+                // them as a set): slots 0,1,2 through index 0; 0,3,4 through 1; 1,3,5 through 2;
+                // 2,4,5 through 3
+                const int bi = J.bi;
+                E.rA0 = bi <= 1 ? J.r[0] : (bi == 2 ? J.r[1] : J.r[2]);
+                E.rA1 = bi == 0 ? J.r[1] : (bi == 3 ? J.r[4] : J.r[3]);
+                E.rA2 = bi == 0 ? J.r[2] : (bi == 1 ? J.r[4] : J.r[5]);
                 E.ncand = J.ncand;
                 E.base = (uint16_t)base; E.L = (uint16_t)J.L; E.H = (uint16_t)J.H;
                 E.E2 = (uint8_t)J.E2;
@@ -655,6 +656,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             }
             // ---- phase B: the pooled candidates, 32 equal contiguous runs
             const uint32_t nc = fits ? J.ncand : 0;
+            const unsigned nonempty = __ballot_sync(FULL, nc != 0);          // jobs with candidates
             uint32_t ci = nc;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
@@ -679,18 +681,18 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
             }
             // the current job of this lane's run, in registers
             uint64_t m64 = 0, m63 = 0, m65 = 0, hv = 0, hc = 0;
-            uint32_t uA = 0, rAA = 0, rAB = 0, rAC1 = 0, rAC2 = 0;
+            uint32_t uA = 0, rAA = 0, rA0 = 0, rA1 = 0, rA2 = 0;
             uint32_t ncand = 0, jb = 0, L = 1, H = 1, E2 = 0, flg = 0, R = 1, dlo = 0, dhi = 0;
             uint32_t cc = 0, l = 0, h = 0, d2 = 0;
             // job fields in four vector loads; entering a job at its first candidate needs no division
             auto load_job = [&](uint32_t j) {
                 const ulonglong2 x0 = *(const ulonglong2 *)&w->job[j].m64;
-                const ulonglong2 x1 = *(const ulonglong2 *)&w->job[j].m65;    // m65, rAB | rAC1 << 32
+                const ulonglong2 x1 = *(const ulonglong2 *)&w->job[j].m65;    // m65, rA0 | rA1 << 32
                 const uint4 y = *(const uint4 *)&w->job[j].uA;
                 const uint2 z = *(const uint2 *)&w->job[j].base;
                 m64 = x0.x; m63 = x0.y; m65 = x1.x;
-                rAB = (uint32_t)x1.y; rAC1 = (uint32_t)(x1.y >> 32);
-                uA = y.x; rAA = y.y; rAC2 = y.z; ncand = y.w;
+                rA0 = (uint32_t)x1.y; rA1 = (uint32_t)(x1.y >> 32);
+                uA = y.x; rAA = y.y; rA2 = y.z; ncand = y.w;
                 jb = z.x & 0xFFFFu; L = z.x >> 16; H = z.y & 0xFFFFu; E2 = (z.y >> 16) & 0xFFu; flg = z.y >> 24;
                 R = (flg & 1) ? E2 - 1 : 1;
                 dlo = flg & 1; dhi = (flg & 1) ? E2 - 1 : 0;      // 2-exponents of f: [1, E2-1] or {0}
@@ -725,7 +727,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     // e = u^2 - A in v (s4.c:197) iff u^2 = A + v_i: u is one of the 4-set's roots
                     // through A (all below 2^23, so u's low word decides once u < 2^32)
                     const uint32_t ul = (uint32_t)u;
-                    const bool member = (u >> 32) == 0 && (ul == rAB || ul == rAC1 || ul == rAC2 || ul == rAA);
+                    const bool member = (u >> 32) == 0 && (ul == rA0 || ul == rA1 || ul == rA2 || ul == rAA);
                     pass = ((m64 >> w64) & (m63 >> w63) & (m65 >> w65) & 1u) && u > uA && !member;
                     if (pass) { sq_run++; cidx = l | (h << 12) | (d2 << 24); }
                     // next candidate of this lane's run
@@ -741,7 +743,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                     if (++cc == ncand && it + 1 < g1 - g0) {
                         if (sq_run) atomicAdd(&w->jsq[jl], sq_run);
                         sq_run = 0;
-                        do { jl++; } while (jl < 31 && w->cstart[jl + 1] == w->cstart[jl]);
+                        jl = min((uint32_t)__ffs(nonempty & (0xFFFFFFFEu << jl)) - 1u, 31u);
                         load_job(jl);
                     }
                 }
