@@ -484,19 +484,31 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
     if ((tid & 31) == 0 && f) atomicAdd(&ts.cnt[K_PAIRS], f);
     __syncthreads();
 
-    // P2: select S with >= 3 representations and S != 2 (mod 4)
-    constexpr uint32_t SEG = L::W / BS;               // even: a thread owns whole counter words
-    const uint32_t i0 = tid * SEG;
+    // P2: select S with >= 3 representations and S != 2 (mod 4).  A thread owns SEG consecutive
+    // S, i.e. WT counter words, and visits them from a lane-dependent rotation so that the lanes
+    // of a warp touch 32 different banks (in plain order they would all hit the same two)
+    constexpr uint32_t SEG = L::W / BS;
+    constexpr uint32_t WT = SEG / 2;
+    static_assert(WT >= 1 && WT <= 32 && (WT & (WT - 1)) == 0, "counter words per thread: a power of two");
+    const uint32_t i0 = tid * SEG, w0 = tid * WT;
+    const uint32_t rot = (((uint32_t)tid & 31u) * WT / 32u) & (WT - 1);
     uint32_t nI = 0, nR = 0, nP = 0, kmax = 0;
     ull trip = 0;
     bool over = false;
-    for (uint32_t i = i0; i < i0 + SEG && i < n; i++) {
-        const uint32_t k = (cnt32[i >> 1] >> ((i & 1) * 16)) & 0xFFFFu;
-        kmax = max(kmax, k);
-        if (k >= 3 && ((S0 + i) & 3) != 2) {
-            nI++; nR += k; nP += k * (k - 1) / 2;
-            trip += (ull)k * (k - 1) * (k - 2) / 6;
-            if (k > a.cap_reps) over = true;
+    for (uint32_t it = 0; it < WT; it++) {
+        const uint32_t wi = (it + rot) & (WT - 1);
+        const uint32_t word = cnt32[w0 + wi];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t i = i0 + 2 * wi + h;
+            const uint32_t k = (word >> (h * 16)) & 0xFFFFu;
+            if (i >= n) continue;
+            kmax = max(kmax, k);
+            if (k >= 3 && ((S0 + i) & 3) != 2) {
+                nI++; nR += k; nP += k * (k - 1) / 2;
+                trip += (ull)k * (k - 1) * (k - 2) / 6;
+                if (k > a.cap_reps) over = true;
+            }
         }
     }
     if (over) raise_error(a.status, E_CAP_REPS, S0);
@@ -523,14 +535,16 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
         ts.cnt[K_S_GE3] += tot[0];
         is_pbase[tot[0]] = tot[2];
     }
-    for (uint32_t i = i0; i < i0 + SEG; i += 2) {
+    for (uint32_t it = 0; it < WT; it++) {
+        const uint32_t wi = (it + rot) & (WT - 1);
+        const uint32_t i = i0 + 2 * wi, cw = cnt32[w0 + wi];
         uint32_t word = 0;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const uint32_t ii = i + h;
             uint32_t val = 0xFFFFu;
             if (ii < n) {
-                const uint32_t k = (cnt32[ii >> 1] >> (h * 16)) & 0xFFFFu;
+                const uint32_t k = (cw >> (h * 16)) & 0xFFFFu;
                 if (k >= 3 && ((S0 + ii) & 3) != 2) {
                     is_off[bI] = (uint16_t)ii; is_k[bI] = (uint16_t)k; is_start[bI] = (uint16_t)bR;
                     is_pbase[bI] = bP;
