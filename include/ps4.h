@@ -282,7 +282,7 @@ typedef struct {
     uint32_t log2_tile;       /* 12 .. 14                                                            */
     uint32_t gen_ctas;        /* 1 .. 2                                                              */
     uint32_t ext_ctas;        /* 1 .. 3                                                              */
-    uint32_t log2_jobs;       /* 20 .. 27                                                            */
+    uint32_t log2_jobs;       /* 20 .. 29                                                            */
     double rate;              /* S/s the tuner measured for this shape (0 if set by hand)            */
 } ps4_tuning;
 

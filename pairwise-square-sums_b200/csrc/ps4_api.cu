@@ -53,14 +53,15 @@ struct ps4_ctx {
     uint64_t *d_raw = nullptr;           // per tile-kernel CTA: SUPER_K tile lists of RAW_PER_TILE
     uint64_t raw_words = 0;
     uint32_t *d_jobs = nullptr;          // 4-set job queue of the two-kernel pipeline (6 x jobs_cap u32)
-    uint64_t jobs_cap = 1ull << 20;          // grows with the calls, up to 2^27 (3.2 GB)
+    uint64_t jobs_cap = 1ull << 20;          // grows with the calls, up to jobs_cap_max
     uint64_t d_jobs_words = 0;
     uint32_t batch_div = 1;              // narrows the batches after a queue overflow
     bool fused_fallback = false;         // this call re-runs on the fused kernel (engine list overflow)
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
     // tuning (ps4_autotune / ps4_set_tuning)
     uint32_t gen_ctas = 2, ext_ctas = 3;     // resident CTAs per SM of the tile kernel / the engine
-    uint64_t jobs_cap_max = 1ull << 27;      // largest job queue (entries)
+    uint64_t jobs_cap_max = 1ull << 29;      // largest job queue (entries; 2^29 = 12.9 GB): fewer,
+                                             //   longer batches, fewer launch tails
     double tuned_rate = 0.0;
     // pinned staging of the segments, and the kept CUDA graph of a multi-batch call
     Item *h_segs = nullptr; uint64_t h_segs_cap = 0;
@@ -678,9 +679,9 @@ extern "C" void ps4_last_transfer_bytes(const ps4_ctx *c, uint64_t *h2d, uint64_
 extern "C" int ps4_set_tuning(ps4_ctx *c, const ps4_tuning *t) {
     if (!c || !t) return PS4_ERR_ARG;
     if (t->log2_tile < 12 || t->log2_tile > 14 || t->gen_ctas < 1 || t->gen_ctas > 2 || t->ext_ctas < 1 ||
-        t->ext_ctas > 3 || t->log2_jobs < 20 || t->log2_jobs > 27)
+        t->ext_ctas > 3 || t->log2_jobs < 20 || t->log2_jobs > 29)
         return set_err(c, PS4_ERR_ARG, "tuning out of range (log2_tile 12..14, gen_ctas 1..2, ext_ctas 1..3, "
-                                       "log2_jobs 20..27)");
+                                       "log2_jobs 20..29)");
     c->tile_log2 = t->log2_tile;
     c->gen_ctas = t->gen_ctas;
     c->ext_ctas = t->ext_ctas;
