@@ -517,7 +517,9 @@ def main():
         "roofline": {"bound": "int_issue", "kernel": dom, "achieved": kernels[dom]["achieved"], "peak": peak,
                      "unit": "lane-op/s", "frac": kernels[dom]["frac"],
                      "peak_source": f"{props.multi_processor_count} SMs x 128 lanes x median SM clock under load "
-                                    f"({sm_hz / 1e6:.0f} MHz sampled); MEASURED_PEAKS.json has no integer peak",
+                                    f"({sm_hz / 1e6:.0f} MHz sampled); " +
+                                    ("MEASURED_PEAKS.json has no integer peak" if (REPO / "MEASURED_PEAKS.json").exists()
+                                     else "no MEASURED_PEAKS.json on this box"),
                      "per": "step (all launches of the kernel in one search of the range; a step is "
                             f"{launches // max(args.steps, 1) // 2} batches)",
                      "ops": kernels[dom]["ops_per_step"], "traffic": kernels[dom]["traffic_per_step"],
