@@ -223,18 +223,21 @@ def measure_triples(local: int, stream, n: int = 10 ** 5, dmax: int = 10 ** 12, 
     return out
 
 
-def measure_serve(local: int, n_req: int, rate: float, seed: int = 20261204, budget: int = 8 << 30) -> dict:
+def measure_serve(local: int, n_req: int, rates, seed: int = 20261204, budget: int = 8 << 30) -> dict:
     """The serving loop on a seeded Poisson stream (70 % subranges, width log-uniform in
-    [1e4, 1e9], offset uniform in [1, 1e12]; 30 % triples, d <= 1e12), replayed in real time;
-    then the same requests in the offline batched form (one batch call, one triple call),
-    with every result compared."""
+    [1e4, 1e9], offset uniform in [1, 1e12]; 30 % triples, d <= 1e12), replayed in real time
+    once per arrival rate (the same requests each time: the seed fixes their contents, the rate
+    only scales the gaps); then the same requests in the offline batched form (one batch call,
+    one triple call), with every result of every stream compared with it."""
     from ps4b200 import Search, workloads
     from ps4b200.serve import Server, run_stream
-    reqs = workloads.requests(n_req, seed=seed, rate=rate)
+    streams, reps = [], []
     with Search(10 ** 12 + 10 ** 9 + 1, device=local) as s:
-        with Server(s, hbm_budget=budget) as srv:
-            run_stream(srv, workloads.requests(20, seed=seed + 7, rate=1000.0, wmax=1e7))     # warm-up
-            rep = run_stream(srv, reqs)
+        for rate in rates:
+            reqs = workloads.requests(n_req, seed=seed, rate=rate)
+            with Server(s, hbm_budget=budget) as srv:
+                run_stream(srv, workloads.requests(20, seed=seed + 7, rate=1000.0, wmax=1e7))     # warm-up
+                reps.append(run_stream(srv, reqs))
         ranges = [r for r in reqs if r.kind == "range"]
         tris = [r for r in reqs if r.kind == "triple"]
         t0 = time.monotonic()
@@ -244,72 +247,117 @@ def measure_serve(local: int, n_req: int, rate: float, seed: int = 20261204, bud
     by_item = {}
     for line, item in zip(res.lines, res.items):
         by_item.setdefault(item, []).append(line)
-    same = True
-    for i, r in enumerate(ranges):
-        g = rep.results[r.rid]
-        same &= (not isinstance(g, Exception)) and g.lines == by_item.get(i, []) and g.stats == stats[i]
-    for i, r in enumerate(tris):
-        g = rep.results[r.rid]
-        same &= (not isinstance(g, Exception)) and g[0] == ext[i] and g[1] == int(state[i])
     S_total = sum(r.hi - r.lo for r in ranges)
-    lat = sorted(rep.latency_s.values())
-    return {"workload": f"{n_req} requests, Poisson at {rate:g}/s, seed {seed}: 70% subranges (width "
-                        f"log-uniform [1e4,1e9], offset uniform [1,1e12]), 30% triples (d <= 1e12)",
-            "p50_ms": 1e3 * rep.percentile(50), "p90_ms": 1e3 * rep.percentile(90),
-            "p99_ms": 1e3 * rep.percentile(99), "max_ms": 1e3 * lat[-1],
-            "requests_per_s": n_req / rep.wall_s, "S_per_s": S_total / rep.wall_s, "wall_s": rep.wall_s,
-            "offline_S_per_s": S_total / off_s, "offline_s": off_s,
-            "identical_to_offline": bool(same),
-            "steps": rep.info["steps"], "step_reruns": rep.info["step_reruns"],
-            "gpu_busy_frac": rep.info["gpu_ms"] / 1e3 / rep.wall_s,
-            "hbm_budget_bytes": budget, "arena_peak_bytes": rep.info["arena_peak"]}
+    all_same = True
+    for rate, rep in zip(rates, reps):
+        same = True
+        for i, r in enumerate(ranges):
+            g = rep.results[r.rid]
+            same &= (not isinstance(g, Exception)) and g.lines == by_item.get(i, []) and g.stats == stats[i]
+        for i, r in enumerate(tris):
+            g = rep.results[r.rid]
+            same &= (not isinstance(g, Exception)) and g[0] == ext[i] and g[1] == int(state[i])
+        all_same &= same
+        lat = sorted(rep.latency_s.values())
+        streams.append({"rate_per_s": rate, "p50_ms": 1e3 * rep.percentile(50), "p90_ms": 1e3 * rep.percentile(90),
+                        "p99_ms": 1e3 * rep.percentile(99), "max_ms": 1e3 * lat[-1],
+                        "requests_per_s": n_req / rep.wall_s, "S_per_s": S_total / rep.wall_s,
+                        "wall_s": rep.wall_s, "steps": rep.info["steps"], "step_reruns": rep.info["step_reruns"],
+                        "gpu_busy_frac": rep.info["gpu_ms"] / 1e3 / rep.wall_s,
+                        "arena_peak_bytes": rep.info["arena_peak"], "identical_to_offline": bool(same)})
+    return {"workload": f"{n_req} requests, Poisson arrivals, seed {seed}: 70% subranges (width "
+                        f"log-uniform [1e4,1e9], offset uniform [1,1e12]), 30% triples (d <= 1e12); the same "
+                        f"requests at each rate",
+            "streams": streams, "S_total": S_total, "offline_S_per_s": S_total / off_s, "offline_s": off_s,
+            "identical_to_offline": bool(all_same), "hbm_budget_bytes": budget}
 
 
-def run_subranges(args, local: int):
-    """The batched uneven-subrange workload as its own line: 4096 subranges (seed 20261203,
-    widths log-uniform in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call, autotuned."""
+CONFIG3_SEED = 20261203
+
+
+def config3_cpu_sample(los, his, budget_s: float = 12.0, seed: int = 5):
+    """The reference's s4 on all host threads over a seeded sample of the 4096 items, each
+    clipped to a centred slice of at most 4e7 S, about budget_s seconds of work in all."""
+    import random
+    binary, kind = _s4_binary()
+    threads = (os.cpu_count() or 1) if kind == "reference" else 1
+    rng = random.Random(seed)
+    order = rng.sample(range(len(los)), len(los))
+    secs, S, n = 0.0, 0, 0
+    for i in order:
+        w = min(his[i] - los[i], 4 * 10 ** 7)
+        a = los[i] + (his[i] - los[i] - w) // 2
+        secs += _run_s4(binary, kind, a, a + w, threads)
+        S += w
+        n += 1
+        if secs >= budget_s:
+            break
+    return {"value": S / secs, "unit": UNIT, "cores": threads, "kind": kind,
+            "sample": f"{n} seeded items of the 4096, each a centred slice of at most 4e7 S ({S} S in all), "
+                      f"slowest region thread's own timer per s4 run"}
+
+
+def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = True) -> dict:
+    """The batched uneven-subrange workload: 4096 subranges (seed 20261203, widths log-uniform
+    in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call, autotuned.  value: S/s from the
+    library's CUDA events around each call's launches; e2e: the same calls timed from the host
+    (pinned inputs copied in, results copied out and formatted)."""
     import torch
     from ps4b200 import Search, workloads
-    los, his = workloads.subranges(4096, seed=20261203)
+    los, his = workloads.subranges(4096, seed=CONFIG3_SEED)
     los, his = los.tolist(), his.tolist()
-    stream = torch.cuda.Stream()
-    torch.cuda.set_stream(stream)
     props = torch.cuda.get_device_properties(local)
     with Search(max(his) + 1, device=local, stream=stream.cuda_stream) as s:
         tune = s.autotune(los, his, budget_s=4.0)
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             s.batch(los, his, want_lines=False)
         clocks = ClockSampler(str(getattr(props, "uuid", "")))
         clocks.start()
         torch.cuda.synchronize()
-        kms, launches = 0.0, 0
+        kms, launches, h2d, d2h = 0.0, 0, 0, 0
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
-            stats, _ = s.batch(los, his, want_lines=False)
+        for _ in range(steps):
+            stats, res = s.batch(los, his, want_lines=True)
             kms += s.last_kernel_ms
             launches += s.last_launches
+            a_, b_ = s.transfer_bytes()
+            h2d += a_
+            d2h += b_
         e1.record(stream)
         torch.cuda.synchronize()
         clk = clocks.stop()
         caps, replays = s.graph_counts()
     S = sum(h - l for l, h in zip(los, his))
-    line = {"metric": METRIC, "value": S * args.steps / (kms / 1e3), "unit": UNIT, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": kms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": {"workload": "4096 uneven subranges, seed 20261203, widths log-uniform in [1e5,1e9], "
-                                   "offsets uniform in [1,1e11], one call = one CUDA graph", "S_total": S,
-                       "tuning": tune, "graphs_captured": caps, "graph_replays": replays},
-            "candidates_per_s": sum(st["ext_cand"] for st in stats) * args.steps / (kms / 1e3),
-            "e2e": {"value": S * args.steps / (e0.elapsed_time(e1) / 1e3), "unit": UNIT},
-            "gpu_launches": launches, "clocks": clk}
+    out = {"workload": "4096 uneven subranges, seed 20261203, widths log-uniform in [1e5,1e9], offsets uniform in "
+                       "[1,1e11], one call = one CUDA graph", "S_total": S,
+           "value": S * steps / (kms / 1e3), "unit": UNIT, "steps": steps, "warmup": warmup,
+           "ms_per_step": kms / steps, "candidates_per_s": sum(st["ext_cand"] for st in stats) * steps / (kms / 1e3),
+           "result_lines": len(res.lines),
+           "e2e": {"value": S * steps / (e0.elapsed_time(e1) / 1e3), "unit": UNIT,
+                   "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps},
+           "tuning": tune, "graphs_captured": caps, "graph_replays": replays,
+           "gpu_launches_per_step": launches // steps, "clocks": clk}
+    if cpu:
+        out["cpu_baseline"] = config3_cpu_sample(los, his)
+    return out
+
+
+def run_subranges(args, local: int):
+    """The batched uneven-subrange workload as its own line."""
+    import torch
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    out = measure_subranges(local, stream, args.steps, args.warmup, cpu=not args.no_cpu_baseline)
+    line = {"metric": METRIC, "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "u64", "data": "synthetic", **out}
     print(json.dumps(line), flush=True)
 
 
 def run_serve(args, local: int):
     import torch
     torch.cuda.set_device(local)
-    out = measure_serve(local, args.serve_requests, args.serve_rate)
+    out = measure_serve(local, args.serve_requests, args.serve_rates)
     print(json.dumps({"metric": "serve_latency_p50_p99", **out}), flush=True)
 
 
@@ -345,9 +393,12 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--workload", choices=["exhaustive", "subranges", "triples", "serve"], default="exhaustive",
                     help="exhaustive: the headline line (S < 1e10); the others print their own line")
-    ap.add_argument("--serve-requests", type=int, default=600)
-    ap.add_argument("--serve-rate", type=float, default=50.0)
+    ap.add_argument("--serve-requests", type=int, default=10000)
+    ap.add_argument("--serve-rates", type=lambda x: [float(v) for v in x.split(",")], default=[50.0, 120.0],
+                    help="arrival rates (requests/s), comma-separated; the same requests at each")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-subranges", action="store_true")
+    ap.add_argument("--subrange-steps", type=int, default=1)
     ap.add_argument("--no-triples", action="store_true")
     ap.add_argument("--range", type=int, nargs=2, default=None, metavar=("LO", "HI"),
                     help="search [LO, HI) instead of the rank's shard (a smaller case for ncu captures)")
@@ -475,12 +526,14 @@ def main():
                "sample": f"{len(slices)} slices of {slices[0][1] - slices[0][0]} S at the midpoints of 4 equal "
                          f"parts of [1,1e10), slowest region thread's own timer"}
 
-    triples = serving = None
+    triples = serving = subranges = None
     if rank == 0 and world == 1 and args.range is None:
         if not args.no_triples:
             triples = measure_triples(local, stream)
+        if not args.no_subranges:
+            subranges = measure_subranges(local, stream, args.subrange_steps, 1, cpu=not args.no_cpu_baseline)
         if not args.no_serve:
-            serving = measure_serve(local, args.serve_requests, args.serve_rate)
+            serving = measure_serve(local, args.serve_requests, args.serve_rates)
 
     if world > 1:
         dist.barrier()
@@ -534,6 +587,7 @@ def main():
         "plain_gpu": plain,
         "cpu_baseline": cpu,
         "triples": triples,
+        "subranges": subranges,
         "serving": serving,
     }
     print(json.dumps(line), flush=True)

@@ -31,6 +31,8 @@ enum {
     PS4_ERR_CAP_DIVS = 11,    /* "divisor capacity exceeded"         (s4.c:176)                    */
     PS4_ERR_CAP_EXT = 12,     /* "extension capacity exceeded"       (s4.c:201)                    */
     PS4_ERR_VERIFY = 13,      /* "quadruple verification failed"     (s4.c:232, --verify only)     */
+    PS4_ERR_CAP_INTERNAL = 14,/* ps4_search_range_noalloc only: a tile's fixed shared-memory list
+                                 overflowed (message names it); the interval is not certified       */
     PS4_ERR_OUTPUT_FULL = 20, /* a caller buffer in ps4_results is too small; n_* hold the needed sizes */
     PS4_ERR_TIMEOUT = 21      /* a device-side bounded wait gave up (persistent kernels, serving)   */
 };
@@ -169,13 +171,37 @@ void ps4_last_transfer_bytes(const ps4_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
  * CTAs plus fixed result buffers of 65536 hits, 131072 extensions and 256 6-sets -- which
  * every GPU that loads the library holds until the process exits.  It rejects, with
  * PS4_ERR_ARG and a message, contexts made with PS4_F_DUMP4 or cap_reps > 512, ranges past
- * the context's s_hi_max and ranges of 2^43 S or more; more records than the fixed buffers
- * hold give PS4_ERR_OUTPUT_FULL (search a shorter range).  The first call on each device
+ * the context's s_hi_max and ranges of 2^43 S or more.  The first call on each device
  * looks up the array's device address (cudaGetSymbolAddress), so make that first call before
- * any stream capture.  Every call on a device shares the array and overwrites it: calls whose
- * work overlaps on the GPU (other threads, other streams) race and must be serialised by the
- * caller.  Synchronous on the context's stream. */
+ * any stream capture; the address is kept per device and looked up again when the device's
+ * primary context has changed (after cudaDeviceReset) or a call failed.  Every call on a device
+ * shares the array and overwrites it: calls whose work overlaps on the GPU (other threads,
+ * other streams) race and must be serialised by the caller.  Synchronous on the context's
+ * stream.
+ *
+ * Errors besides the regular search's: more records than the fixed buffers hold give
+ * PS4_ERR_OUTPUT_FULL with n_* set to the counts the search produced (at least one above its
+ * PS4_NOALLOC_MAX_* limit; nothing is copied; search a shorter range).  A tile whose lists
+ * outgrow their fixed shared-memory sizes gives PS4_ERR_CAP_INTERNAL: a capacity failure that a
+ * shorter range does not avoid, reported like the reference's FATAL lines (interval not
+ * certified complete). */
+#define PS4_NOALLOC_MAX_HITS 65536u
+#define PS4_NOALLOC_MAX_EXTS 131072u
+#define PS4_NOALLOC_MAX_SIXES 256u
 int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res);
+
+/* ---- exact-root self-check ----
+ *
+ * Runs the device's exact integer square roots -- the routines every square test and tile
+ * scan of the search uses, restating isqrt64 / isqrt128 / is_sq128 (exhaustive/s4.c:95-108) --
+ * on n[i] = hi[i]*2^64 + lo[i], so that they can be checked against exact host arithmetic
+ * at their edges.  roots[4i..4i+3] = floor(sqrt(n)) (128-bit), floor(sqrt(lo)), ceil(sqrt(lo)),
+ * and floor(sqrt(lo)) by the tile scan's single-precision estimate (lo < 2^46, else 0);
+ * flags[i] bit 0: n is a square (exact test), bit 1: n is a square by the search's fast test,
+ * evaluated only for n < 2^100, its precondition (else 0).  Allocates and frees its own device
+ * buffers on `device`; synchronous. */
+int ps4_check_roots(int device, const uint64_t *lo, const uint64_t *hi, uint32_t n, uint64_t *roots,
+                    uint32_t *flags);
 
 /* ---- triple extension ----
  *

@@ -458,7 +458,6 @@ static int enqueue_items(ps4_ctx *c) {
             if (e == cudaSuccess) e = e2;
             if (e == cudaSuccess) {
                 if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
-    for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
                 c->graph_exec = nullptr;
                 c->graph_key.clear();
                 e = cudaGraphInstantiate(&c->graph_exec, g, 0);

@@ -30,6 +30,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "ps4_internal.h"
 
@@ -294,6 +295,25 @@ __global__ void build_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t n) {
     }
 }
 
+// ================================================================== exact-root self-check
+
+// The search's exact roots on n = hi*2^64 + lo, one thread per value (ps4_check_roots):
+// out[4i..4i+3] = isqrt128(n), isqrt64(lo), ceil_sqrt64(lo), isqrt_lt2p46(lo) (the last only
+// for lo < 2^46, else 0); flags[i] bit 0 = is_square_exact(n), bit 1 = is_square_fast(n) (only
+// for n < 2^100, its precondition; else 0).
+__global__ void check_roots(const uint64_t *lo, const uint64_t *hi, uint32_t n, uint64_t *out, uint32_t *flags) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u128 x = ((u128)hi[i] << 64) | lo[i];
+    out[4 * (size_t)i + 0] = isqrt128(x);
+    out[4 * (size_t)i + 1] = isqrt64(lo[i]);
+    out[4 * (size_t)i + 2] = ceil_sqrt64(lo[i]);
+    out[4 * (size_t)i + 3] = lo[i] < (1ull << 46) ? isqrt_lt2p46(lo[i]) : 0ull;
+    uint32_t f = is_square_exact(x) ? 1u : 0u;
+    if ((x >> 100) == 0 && is_square_fast(x)) f |= 2u;
+    flags[i] = f;
+}
+
 // ================================================================== launchers
 
 int search_block_threads() { return BS; }
@@ -342,6 +362,33 @@ int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream) 
 
 }  // namespace ps4
 
+// Self-check of the device's exact roots (no context: device buffers of its own, synchronous).
+extern "C" int ps4_check_roots(int device, const uint64_t *lo, const uint64_t *hi, uint32_t n, uint64_t *roots,
+                               uint32_t *flags) {
+    if (n == 0) return PS4_OK;
+    if (!lo || !hi || !roots || !flags) return PS4_ERR_ARG;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return PS4_ERR_CUDA;
+    uint64_t *d_in = nullptr, *d_out = nullptr;
+    uint32_t *d_flags = nullptr;
+    cudaError_t e = cudaMalloc((void **)&d_in, 2 * (size_t)n * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_out, 4 * (size_t)n * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_flags, (size_t)n * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpy(d_in, lo, (size_t)n * sizeof(uint64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d_in + n, hi, (size_t)n * sizeof(uint64_t), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        ps4::check_roots<<<(n + 255) / 256, 256>>>(d_in, d_in + n, n, d_out, d_flags);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(roots, d_out, 4 * (size_t)n * sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(flags, d_flags, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    cudaFree(d_in);
+    cudaFree(d_out);
+    cudaFree(d_flags);
+    if (prev != device) cudaSetDevice(prev);
+    return e == cudaSuccess ? PS4_OK : PS4_ERR_CUDA;
+}
+
 // ================================================================== allocation-free variant
 //
 // ps4_search_range_noalloc (include/ps4.h) runs a variant of the batched kernel whose only
@@ -353,7 +400,7 @@ namespace noalloc {
 constexpr int TL = 12;                        // S values per tile: 4096
 constexpr uint32_t CTAS = 148;                // at most one CTA per SM of a B200
 constexpr uint32_t STAGE = 16384;             // staged 4-sets per CTA
-constexpr uint32_t HITS = 65536, EXTS = 131072, SIXES = 256;
+constexpr uint32_t HITS = PS4_NOALLOC_MAX_HITS, EXTS = PS4_NOALLOC_MAX_EXTS, SIXES = PS4_NOALLOC_MAX_SIXES;
 constexpr size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 constexpr size_t OFF_STAGE = 0;
 constexpr size_t OFF_STATUS = al(OFF_STAGE + (size_t)CTAS * 6 * STAGE * sizeof(uint32_t));
@@ -482,6 +529,59 @@ __global__ void __launch_bounds__(BS, 1) search_batched_fixed(const SearchArgs a
 // with the library's device code on every GPU that runs it, held until the process exits.
 static __device__ __align__(256) unsigned char ps4_noalloc_scratch[ps4::noalloc::BYTES];
 
+namespace {
+// The device address of ps4_noalloc_scratch on each device, with the primary context it was
+// looked up in.  Host code only ever holds the array's host-side stand-in; a kernel must be
+// given the address looked up here.  Guarded by a mutex: two host threads may make their
+// first calls on a device at the same time.
+struct NoallocBase {
+    void *cu_ctx = nullptr;
+    void *base = nullptr;
+};
+std::mutex noalloc_mu;
+NoallocBase noalloc_base[64];
+
+// The calling thread's current CUDA context (the device's primary context once the runtime
+// has set the device up), through the driver entry point the runtime hands out: nullptr if
+// it cannot be had, in which case the cached address is trusted as it is.
+void *current_cu_ctx() {
+    typedef int (*get_ctx_t)(void **);
+    static const get_ctx_t fn = []() -> get_ctx_t {
+        void *f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return (get_ctx_t)f;
+    }();
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
+
+// The array's address on `device` (current): looked up once per device and primary context.
+cudaError_t noalloc_base_of(int device, void **out) {
+    std::lock_guard<std::mutex> lock(noalloc_mu);
+    NoallocBase &nb = noalloc_base[device];
+    void *ctx = current_cu_ctx();
+    if (!nb.base || (ctx && ctx != nb.cu_ctx)) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, ps4_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        nb.base = p;
+        nb.cu_ctx = ctx ? ctx : current_cu_ctx();
+    }
+    *out = nb.base;
+    return cudaSuccess;
+}
+
+// After a failed call the next one looks the address up again.
+void noalloc_forget(int device) {
+    std::lock_guard<std::mutex> lock(noalloc_mu);
+    noalloc_base[device] = NoallocBase();
+}
+}  // namespace
+
 extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res) {
     using namespace ps4;
     namespace na = ps4::noalloc;
@@ -501,29 +601,27 @@ extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, 
         return ctx_fail(ctx, PS4_ERR_ARG, "ps4_search_range_noalloc: range too large for one call; split it");
     res->n_hits = res->n_exts = res->n_sixes = res->n_quads = 0;
     if (n_tiles == 0) return PS4_OK;
-
-    // Once per device, with that device current: the device address of the static array.
-    // (The host-side name ps4_noalloc_scratch is only a stand-in and must not reach a kernel.)
-    static void *base_of[64];
     if (v.device < 0 || v.device >= 64) return ctx_fail(ctx, PS4_ERR_ARG, "device ordinal out of range");
+
     int prev = 0;
     if (cudaGetDevice(&prev) != cudaSuccess) return ctx_fail(ctx, PS4_ERR_CUDA, "cudaGetDevice failed");
     if (prev != v.device && cudaSetDevice(v.device) != cudaSuccess)
         return ctx_fail(ctx, PS4_ERR_CUDA, "cudaSetDevice failed");
     int rc = PS4_OK;
-    char msg[256];
+    bool cuda_failed = false;
+    char msg[320];
     do {
-        if (!base_of[v.device]) {
-            void *p = nullptr;
-            cudaError_t e = cudaGetSymbolAddress(&p, ps4_noalloc_scratch);
-            if (e != cudaSuccess) {
-                snprintf(msg, sizeof msg, "cudaGetSymbolAddress(ps4_noalloc_scratch) failed: %s", cudaGetErrorString(e));
-                rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
-                break;
-            }
-            base_of[v.device] = p;
+        // once per device (and primary context), with that device current: the device address
+        // of the static array -- the host-side name ps4_noalloc_scratch must not reach a kernel
+        void *basep = nullptr;
+        cudaError_t e = noalloc_base_of(v.device, &basep);
+        if (e != cudaSuccess) {
+            snprintf(msg, sizeof msg, "cudaGetSymbolAddress(ps4_noalloc_scratch) failed: %s", cudaGetErrorString(e));
+            rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
+            cuda_failed = true;
+            break;
         }
-        unsigned char *base = (unsigned char *)base_of[v.device];
+        unsigned char *base = (unsigned char *)basep;
         Status *d_status = (Status *)(base + na::OFF_STATUS);
         unsigned long long *d_counters = (unsigned long long *)(base + na::OFF_COUNTERS);
         Item *d_item = (Item *)(base + na::OFF_ITEM);
@@ -545,7 +643,7 @@ extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, 
         const unsigned grid = (unsigned)std::min<uint64_t>(std::min<uint64_t>(na::CTAS, (uint64_t)v.num_sms), n_tiles);
         const size_t smem = TileLayout<na::TL>::BYTES;
         // what must start at zero: the status (error word, record counts, tile counter) and the counters
-        cudaError_t e = cudaMemcpyAsync(d_item, &it, sizeof it, cudaMemcpyHostToDevice, s);
+        e = cudaMemcpyAsync(d_item, &it, sizeof it, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaMemsetAsync(d_status, 0, sizeof(Status), s);
         if (e == cudaSuccess) e = cudaMemsetAsync(d_counters, 0, K_SLOTS * sizeof(unsigned long long), s);
         if (e == cudaSuccess)
@@ -560,12 +658,13 @@ extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, 
         if (e != cudaSuccess) {
             snprintf(msg, sizeof msg, "ps4_search_range_noalloc: %s", cudaGetErrorString(e));
             rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
+            cuda_failed = true;
             break;
         }
         const unsigned code = (unsigned)(st.err & 0xFF);
+        const unsigned long long errS = st.err >> 8;
         if (code == E_CAP_REPS || code == E_CAP_DIVS || code == E_CAP_EXT) {
-            const char *what = code == E_CAP_REPS ? "representation" : code == E_CAP_DIVS ? "divisor" : "extension";
-            snprintf(msg, sizeof msg, "FATAL: %s capacity exceeded; this interval is NOT certified complete", what);
+            snprintf(msg, sizeof msg, "FATAL: %s; this interval is NOT certified complete", fatal_text(code));
             rc = ctx_fail(ctx, (int)code, msg);
             break;
         }
@@ -577,18 +676,28 @@ extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, 
             break;
         }
         if (code != 0) {
-            snprintf(msg, sizeof msg, "ps4_search_range_noalloc: a tile near S=%llu outgrew the fixed shared-memory "
-                     "lists; search it with ps4_search_range", st.err >> 8);
-            rc = ctx_fail(ctx, PS4_ERR_CAP_REPS, msg);
-            break;
-        }
-        if (st.n_hits > na::HITS || st.n_exts > na::EXTS || st.n_sixes > na::SIXES) {
-            snprintf(msg, sizeof msg, "ps4_search_range_noalloc: %u result records exceed the fixed buffers "
-                     "(%u hits); search a shorter range", st.n_hits, na::HITS);
-            rc = ctx_fail(ctx, PS4_ERR_OUTPUT_FULL, msg);
+            // a tile's fixed shared-memory list (selected S, representations, 4-set staging or
+            // extension list) overflowed: the tile's size is fixed here, so a shorter range meets
+            // the same tile again
+            static const char *list_name[5] = {"?", "selected-S list", "representation list", "4-set staging",
+                                               "extension list"};
+            snprintf(msg, sizeof msg,
+                     "FATAL: internal capacity exceeded near S=%llu (%s: %llu > %llu); this interval is NOT "
+                     "certified complete", errS, list_name[st.diag[0] < 5 ? st.diag[0] : 0], st.diag[1], st.diag[2]);
+            rc = ctx_fail(ctx, PS4_ERR_CAP_INTERNAL, msg);
             break;
         }
         res->n_hits = st.n_hits; res->n_exts = st.n_exts; res->n_sixes = st.n_sixes;
+        if (st.n_hits > na::HITS || st.n_exts > na::EXTS || st.n_sixes > na::SIXES) {
+            snprintf(msg, sizeof msg,
+                     "ps4_search_range_noalloc: the fixed result buffers overflowed (%s%s%s): hits %u of %u, "
+                     "extensions %u of %u, 6-sets %u of %u; nothing was copied, search a shorter range",
+                     st.n_hits > na::HITS ? "hits " : "", st.n_exts > na::EXTS ? "extensions " : "",
+                     st.n_sixes > na::SIXES ? "6-sets" : "", st.n_hits, na::HITS, st.n_exts, na::EXTS, st.n_sixes,
+                     na::SIXES);
+            rc = ctx_fail(ctx, PS4_ERR_OUTPUT_FULL, msg);
+            break;
+        }
         if (res->n_hits > res->hits_cap || res->n_exts > res->exts_cap || res->n_sixes > res->sixes_cap) {
             rc = ctx_fail(ctx, PS4_ERR_OUTPUT_FULL, "ps4_search_range_noalloc: result buffers too small; n_* hold the sizes");
             break;
@@ -605,15 +714,12 @@ extern "C" int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, 
         if (e != cudaSuccess) {
             snprintf(msg, sizeof msg, "ps4_search_range_noalloc: %s", cudaGetErrorString(e));
             rc = ctx_fail(ctx, PS4_ERR_CUDA, msg);
+            cuda_failed = true;
             break;
         }
-        uint64_t *add = &stats->S_done;
-        for (int i = 0; i < 10; i++) add[i] += k[i];
-        for (int i = 0; i < 100; i++) stats->hist5[i] += k[K_HIST5 + i];
-        stats->max_reps = std::max<uint64_t>(stats->max_reps, k[K_MAX_REPS]);
-        stats->max_divisors = std::max<uint64_t>(stats->max_divisors, k[K_MAX_DIVS]);
-        stats->max_extensions = std::max<uint64_t>(stats->max_extensions, k[K_MAX_EXT]);
+        stats_add(stats, k);
     } while (0);
+    if (cuda_failed) noalloc_forget(v.device);
     if (prev != v.device) cudaSetDevice(prev);
     return rc;
 }

@@ -21,8 +21,14 @@ PS4_ERR_CAP_REPS = 10
 PS4_ERR_CAP_DIVS = 11
 PS4_ERR_CAP_EXT = 12
 PS4_ERR_VERIFY = 13
+PS4_ERR_CAP_INTERNAL = 14
 PS4_ERR_OUTPUT_FULL = 20
 PS4_ERR_TIMEOUT = 21
+
+# fixed result buffers of ps4_search_range_noalloc
+PS4_NOALLOC_MAX_HITS = 65536
+PS4_NOALLOC_MAX_EXTS = 131072
+PS4_NOALLOC_MAX_SIXES = 256
 
 PS4_F_NOEXT = 1
 PS4_F_VERIFY = 2
@@ -136,6 +142,8 @@ def load() -> C.CDLL:
                                        P(Results)]),
         "ps4_search_range_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, P(Stats), P(Results)]),
         "ps4_search_enqueue": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
+        "ps4_check_roots": (C.c_int, [C.c_int, P(C.c_uint64), P(C.c_uint64), C.c_uint32, P(C.c_uint64),
+                                      P(C.c_uint32)]),
         "ps4_search_finish": (C.c_int, [C.c_void_p, P(Stats), P(Results)]),
         "ps4_last_transfer_bytes": (None, [C.c_void_p, P(C.c_uint64), P(C.c_uint64)]),
         "ps4_extend_triples": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p, C.c_void_p,

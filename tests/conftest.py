@@ -7,6 +7,7 @@ from __future__ import annotations
 
 import gzip
 import json
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -33,6 +34,19 @@ def _ensure_built():
 
 
 _ensure_built()
+
+
+def reference_tree():
+    """The reference's source tree, where tests read its own modules and evidence: the
+    PS4_REFERENCE_TREE environment variable, else the directory `make -C oracle ref` recorded in
+    oracle/_ref/REF_DIR when it built the reference binary; None when neither names one that
+    exists (on a GPU box the tree is absent and those tests skip)."""
+    env = os.environ.get("PS4_REFERENCE_TREE")
+    cand = Path(env) if env else None
+    rec = REPO / "oracle" / "_ref" / "REF_DIR"
+    if cand is None and rec.exists():
+        cand = Path(rec.read_text().strip())
+    return cand if cand is not None and (cand / "exhaustive").is_dir() else None
 
 
 @pytest.fixture(scope="session")

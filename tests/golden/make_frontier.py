@@ -3,7 +3,7 @@
 archives (exhaustive/evidence/exhaustive-2026-09-18.tar.gz and -09-19.tar.gz, S ~ 1.95e12 to
 3.5e12) -- their sorted-output sha256, M lines and TOTAL counters -- into frontier.json.
 
-    python tests/golden/make_frontier.py [/path/to/reference]
+    python tests/golden/make_frontier.py REFERENCE_TREE
 """
 from __future__ import annotations
 
@@ -19,7 +19,10 @@ from make_golden import parse_stderr, sha  # noqa: E402
 
 
 def main() -> int:
-    ref = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        print(__doc__, file=sys.stderr)
+        return 2
+    ref = Path(sys.argv[1])
     blocks = []
     for arch, picks in (("exhaustive-2026-09-18", (40, 80, 120, 155)), ("exhaustive-2026-09-19", (1, 60, 110, 159))):
         with tarfile.open(ref / "exhaustive" / "evidence" / f"{arch}.tar.gz") as tar:

@@ -3,10 +3,10 @@
 
 Runs oracle/_ref/s4 -- the reference's exhaustive/s4.c compiled unmodified by
 `make -C oracle ref` -- and reads the reference's own logs and unit-test vectors from the
-reference tree.  Needs the reference tree (default /root/reference); the fixtures it writes
+reference tree.  Needs the reference tree (--ref); the fixtures it writes
 are committed, so the tests never need the reference at run time.
 
-    python tests/golden/make_golden.py [--ref /root/reference] [--reuse DIR] [--skip-1e10]
+    python tests/golden/make_golden.py --ref REFERENCE_TREE [--reuse DIR] [--skip-1e10]
 
 --reuse DIR takes s4_1e9.{out,err} / s4_1e10.{out,err} already produced by
 `s4 1 1000000000 8 20` / `s4 1 10000000000 8 20` in DIR instead of re-running them
@@ -73,7 +73,7 @@ def random_subranges(seed: int, n: int):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="the reference source tree")
     ap.add_argument("--reuse", default=None)
     ap.add_argument("--skip-1e10", action="store_true")
     args = ap.parse_args()

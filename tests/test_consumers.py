@@ -17,12 +17,12 @@ from pathlib import Path
 import pytest
 
 import consumers
-from conftest import GOLDEN_DIR
+from conftest import GOLDEN_DIR, reference_tree
 from golden.make_golden import parse_stderr
 
 BLOCK = GOLDEN_DIR / "cli_block"
-REF_TREE = Path(os.environ.get("PS4_REFERENCE_TREE", "/root/reference"))
-HAVE_REF = (REF_TREE / "exhaustive" / "verify.py").is_file()
+REF_TREE = reference_tree()
+HAVE_REF = REF_TREE is not None and (REF_TREE / "exhaustive" / "verify.py").is_file()
 CONTROLLER_ARCHIVE = "exhaustive-2026-10-13-8h-compact.tar.gz"
 needs_ref = pytest.mark.skipif(not HAVE_REF, reason="the reference tree is not present")
 
