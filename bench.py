@@ -3,11 +3,12 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--kernel batched|plain]
 
-One step = one complete search of the rank's S range (the reference's `s4 1 10000000000`):
-every 4-set with S below the bound, every extension, every counter.  N > 1 runs under
-torchrun, one process per GPU; each rank searches its own 1e10-wide shard
-[r*1e10, (r+1)*1e10) (weak scaling, no data-path collective; the time is the max over
-ranks).  Rank 0 prints one JSON line.
+One step = one complete search of S in [1, 1e10) (the reference's `s4 1 10000000000`): every
+4-set with S below the bound, every extension, every counter.  N > 1 runs under torchrun, one
+process per GPU; the same range is cut into N contiguous shards of about equal search cost
+(ps4b200.shards.plan, the library's ps4_plan_shards), each rank searches its shard (strong
+scaling, no data-path collective; the time is the max over ranks; the e2e leg gathers the
+shards' results on the host).  Rank 0 prints one JSON line.
 
 value      S covered per second with the work enqueued on the device (CUDA events on the
            launch stream around each step; a 256 MiB write flushes L2 between steps,
@@ -41,9 +42,11 @@ METRIC = "range_per_s"
 UNIT = "S/s"
 
 
-def shard(rank: int, bound: int = BOUND) -> tuple[int, int]:
-    """Rank r searches S in [max(1, r*B), (r+1)*B): rank 0 is the s4 bound-1e10 workload."""
-    return max(1, rank * bound), (rank + 1) * bound
+def shard(rank: int, world: int, bound: int = BOUND) -> tuple[int, int]:
+    """Rank r's shard of S in [1, bound): contiguous, about equal search cost per rank."""
+    from ps4b200 import shards
+    b = shards.plan(1, bound, world)
+    return b[rank], b[rank + 1]
 
 
 def aggregate(dist, world: int, times: list, totals: list, device) -> tuple[list, list]:
@@ -110,7 +113,7 @@ def run_reference(args, rank: int):
     """The reference arm: s4 itself on this host's cores, on a bounded sample of the workload."""
     if rank != 0:
         return
-    lo, hi = shard(0)
+    lo, hi = 1, BOUND
     binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=args.ref_budget)
     for _ in range(args.warmup):
         cpu_sample_run(binary, kind, threads, slices)
@@ -123,7 +126,7 @@ def run_reference(args, rank: int):
     sample = f"{len(slices)} slices of {slices[0][1] - slices[0][0]} S at the midpoints of 4 equal parts of [1,1e10)"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * total_s / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "exhaustive",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "exhaustive",
             "config": {"workload": "exhaustive square-sum search, S in [1,1e10) (s4 bound 1e10), sampled",
                        "bound": BOUND, "sample": sample},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind, "sample": sample},
@@ -426,12 +429,12 @@ def main():
     import torch
     import torch.distributed as dist
     from datetime import timedelta
-    from ps4b200 import Search, opmodel
+    from ps4b200 import Search, opmodel, shards
 
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
-    lo, hi = shard(rank) if args.range is None else tuple(args.range)
+    lo, hi = shard(rank, world) if args.range is None else tuple(args.range)
     # one dedicated stream carries the library's launches, the L2 flush and the timing events
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -479,7 +482,10 @@ def main():
     h2d = d2h = 0
     e2e_lines = 0
     for _ in range(args.steps):
-        rr = s.range(lo, hi)
+        if args.range is None:             # the whole range: this rank's shard, results gathered
+            rr, _ = shards.search_sharded(1, BOUND, rank=rank, world=world, dist=dist, search=s)
+        else:
+            rr = s.range(lo, hi)
         a_, b_ = s.transfer_bytes()
         h2d += a_
         d2h += b_
@@ -559,11 +565,11 @@ def main():
     line = {
         "metric": METRIC, "value": S_all / dev_s, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * dev_s / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "exhaustive",
-        "config": {"workload": "exhaustive square-sum 4-set search + extension, S in [r*1e10, (r+1)*1e10) "
-                               "per rank (s4 bound 1e10 on rank 0)",
-                   "bound_per_rank": BOUND, "kernel": args.kernel, "l2": "256 MiB write between timed steps",
-                   "parallelism": f"S shards x{world}"},
+        "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "exhaustive",
+        "config": {"workload": "exhaustive square-sum 4-set search + extension, S in [1,1e10) (s4 bound 1e10)"
+                               + (f", {world} cost-balanced contiguous S shards, one per GPU" if world > 1 else ""),
+                   "bound": BOUND, "shard": [lo, hi], "kernel": args.kernel,
+                   "l2": "256 MiB write between timed steps", "parallelism": f"S shards x{world}"},
         "candidates_per_s": cand_all / dev_s,
         "sets4_per_s": stats["sets4"] * world * args.steps / dev_s,
         "kernel_ms_per_step": 1000 * kern_s / args.steps,

@@ -190,6 +190,21 @@ void ps4_last_transfer_bytes(const ps4_ctx *ctx, uint64_t *h2d, uint64_t *d2h);
 #define PS4_NOALLOC_MAX_SIXES 256u
 int ps4_search_range_noalloc(ps4_ctx *ctx, uint64_t lo, uint64_t hi, ps4_stats *stats, ps4_results *res);
 
+/* ---- one range on several devices ----
+ *
+ * Cut [lo, hi) into n contiguous shards of about equal search cost, for n devices (one
+ * process or context each) searching one range.  Every result line and counter of the search
+ * is a function of S alone (exhaustive/s4.c:313-341), so the shards' result lines concatenate
+ * in shard order into the whole range's canonical order, and their counters add (the three
+ * CAPACITY maxima take the maximum).  Replaces the reference's equal-width split of [S_lo,
+ * S_hi) into thread regions (exhaustive/s4.c:452-456): the search's cost per S grows with S,
+ * so equal widths leave the top shard the slowest.  The cost model is a density proportional
+ * to S^0.16, fitted to this library's measured rates (5.5e-11 s per S averaged over [1,1e10),
+ * 1.2e-10 s per S near 5e11); shard i is [bounds[i], bounds[i+1]) with bounds[0] = max(lo, 1),
+ * bounds[n] = hi, and inner bounds on multiples of 2^14 S (one tile).  Host only (no device).
+ * bounds holds n + 1 values; n >= 1. */
+int ps4_plan_shards(uint64_t lo, uint64_t hi, uint32_t n, uint64_t *bounds);
+
 /* ---- exact-root self-check ----
  *
  * Runs the device's exact integer square roots -- the routines every square test and tile

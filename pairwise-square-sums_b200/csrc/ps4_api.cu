@@ -673,6 +673,28 @@ extern "C" void ps4_last_transfer_bytes(const ps4_ctx *c, uint64_t *h2d, uint64_
     if (d2h) *d2h = c ? c->d2h_bytes : 0;
 }
 
+// ---- one range on several devices ----
+
+extern "C" int ps4_plan_shards(uint64_t lo, uint64_t hi, uint32_t n, uint64_t *bounds) {
+    if (n == 0 || !bounds) return PS4_ERR_ARG;
+    lo = std::max<uint64_t>(lo, 1);
+    hi = std::max(hi, lo);
+    // cumulative cost C(S) = S^(1+beta): density ~ S^beta, beta fitted to the measured rates
+    const double beta = 0.16, g = 1.0 + beta;
+    const double c0 = std::pow((double)lo, g), c1 = std::pow((double)hi, g);
+    const uint64_t tile = 1ull << 14;
+    bounds[0] = lo;
+    for (uint32_t i = 1; i < n; i++) {
+        const double x = std::pow(c0 + (c1 - c0) * (double)i / (double)n, 1.0 / g);
+        uint64_t b = x <= (double)lo ? lo : x >= (double)hi ? hi : (uint64_t)x;
+        b = (b + tile / 2) / tile * tile;                   // nearest tile boundary
+        b = std::min(hi, std::max(b, bounds[i - 1]));
+        bounds[i] = b;
+    }
+    bounds[n] = hi;
+    return PS4_OK;
+}
+
 // ---- tuning ----
 
 extern "C" int ps4_set_tuning(ps4_ctx *c, const ps4_tuning *t) {

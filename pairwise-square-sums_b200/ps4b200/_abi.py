@@ -142,6 +142,7 @@ def load() -> C.CDLL:
                                        P(Results)]),
         "ps4_search_range_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, P(Stats), P(Results)]),
         "ps4_search_enqueue": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
+        "ps4_plan_shards": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, P(C.c_uint64)]),
         "ps4_check_roots": (C.c_int, [C.c_int, P(C.c_uint64), P(C.c_uint64), C.c_uint32, P(C.c_uint64),
                                       P(C.c_uint32)]),
         "ps4_search_finish": (C.c_int, [C.c_void_p, P(Stats), P(Results)]),
