@@ -300,18 +300,21 @@ def config3_cpu_sample(los, his, budget_s: float = 12.0, seed: int = 5):
                       f"slowest region thread's own timer per s4 run"}
 
 
-def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = True) -> dict:
+def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = True, kernel: str = "persist",
+                      compare: str | None = "batched") -> dict:
     """The batched uneven-subrange workload: 4096 subranges (seed 20261203, widths log-uniform
-    in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call, autotuned.  value: S/s from the
+    in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call: on the persistent kernel, one
+    launch over a ring of 4-sets, or on the two-kernel pipeline, autotuned.  value: S/s from the
     library's CUDA events around each call's launches; e2e: the same calls timed from the host
-    (pinned inputs copied in, results copied out and formatted)."""
+    (pinned inputs copied in, results copied out and formatted).  `compare`: the other kernel,
+    one step, its rate and whether every item's counters and lines equal."""
     import torch
     from ps4b200 import Search, workloads
     los, his = workloads.subranges(4096, seed=CONFIG3_SEED)
     los, his = los.tolist(), his.tolist()
     props = torch.cuda.get_device_properties(local)
-    with Search(max(his) + 1, device=local, stream=stream.cuda_stream) as s:
-        tune = s.autotune(los, his, budget_s=4.0)
+    with Search(max(his) + 1, device=local, stream=stream.cuda_stream, kernel=kernel) as s:
+        tune = s.autotune(los, his, budget_s=4.0) if kernel == "batched" else None
         for _ in range(warmup):
             s.batch(los, his, want_lines=False)
         clocks = ClockSampler(str(getattr(props, "uuid", "")))
@@ -333,7 +336,7 @@ def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = T
         caps, replays = s.graph_counts()
     S = sum(h - l for l, h in zip(los, his))
     out = {"workload": "4096 uneven subranges, seed 20261203, widths log-uniform in [1e5,1e9], offsets uniform in "
-                       "[1,1e11], one call = one CUDA graph", "S_total": S,
+                       "[1,1e11], one call = one CUDA graph", "S_total": S, "kernel": kernel,
            "value": S * steps / (kms / 1e3), "unit": UNIT, "steps": steps, "warmup": warmup,
            "ms_per_step": kms / steps, "candidates_per_s": sum(st["ext_cand"] for st in stats) * steps / (kms / 1e3),
            "result_lines": len(res.lines),
@@ -341,6 +344,15 @@ def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = T
                    "h2d_bytes_per_step": h2d // steps, "d2h_bytes_per_step": d2h // steps},
            "tuning": tune, "graphs_captured": caps, "graph_replays": replays,
            "gpu_launches_per_step": launches // steps, "clocks": clk}
+    if compare:
+        with Search(max(his) + 1, device=local, stream=stream.cuda_stream, kernel=compare) as o:
+            otune = o.autotune(los, his, budget_s=4.0) if compare == "batched" else None
+            ostats, ores = o.batch(los, his, want_lines=True)
+            out["compare"] = {"kernel": compare, "value": S / (o.last_kernel_ms / 1e3), "unit": UNIT,
+                              "ms_per_step": o.last_kernel_ms, "gpu_launches_per_step": o.last_launches,
+                              "tuning": otune,
+                              "identical": ostats == stats and sorted(zip(ores.items, ores.lines)) ==
+                              sorted(zip(res.items, res.lines))}
     if cpu:
         out["cpu_baseline"] = config3_cpu_sample(los, his)
     return out

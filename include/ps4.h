@@ -49,7 +49,11 @@ enum {
     PS4_KERNEL_BATCHED = 0, /* per batch of S: persistent tile kernel queues every 4-set, then the
                                extension engine pools their divisor pairs warp-wide (default)        */
     PS4_KERNEL_PLAIN = 1,   /* one CTA per tile, one thread per S, inline extension (baseline)       */
-    PS4_KERNEL_FUSED = 2    /* one persistent kernel: tiles, staging and per-lane extension fused    */
+    PS4_KERNEL_FUSED = 2,   /* one persistent kernel: tiles, staging and per-lane extension fused    */
+    PS4_KERNEL_PERSIST = 3  /* one launch per call over every subrange: CTAs switch between writing
+                               tiles' 4-sets into a device ring and running the extension engine on
+                               the ring; falls back to PS4_KERNEL_BATCHED when one of its bounded
+                               waits gives up                                                          */
 };
 
 typedef struct ps4_ctx ps4_ctx;
@@ -217,6 +221,14 @@ int ps4_plan_shards(uint64_t lo, uint64_t hi, uint32_t n, uint64_t *bounds);
  * buffers on `device`; synchronous. */
 int ps4_check_roots(int device, const uint64_t *lo, const uint64_t *hi, uint32_t n, uint64_t *roots,
                     uint32_t *flags);
+
+/* Self-check of the bounded waits of PS4_KERNEL_PERSIST: one device thread waits, as a consuming
+ * warp does, for a ring position that nothing publishes.  The wait gives up after its time limit
+ * (2 s) and records the timeout instead of spinning on; the call returns PS4_ERR_TIMEOUT when that
+ * happened as designed (PS4_OK would mean the wait ended otherwise) and *waited_ns the time it
+ * waited.  No counterpart in the reference (its threads never wait on one another).  Allocates
+ * and frees its own small device buffers on `device`; synchronous. */
+int ps4_check_ring_wait(int device, uint64_t *waited_ns);
 
 /* ---- triple extension ----
  *

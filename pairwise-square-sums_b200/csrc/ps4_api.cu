@@ -57,6 +57,11 @@ struct ps4_ctx {
     uint64_t d_jobs_words = 0;
     uint32_t batch_div = 1;              // narrows the batches after a queue overflow
     bool fused_fallback = false;         // this call re-runs on the fused kernel (engine list overflow)
+    bool persist_fallback = false;       // this call re-runs on the two-kernel pipeline (a persistent-kernel
+                                         //   wait gave up, or a tile outgrew the 2^13-S tile lists)
+    uint32_t *d_seq = nullptr;           // the persistent kernel's ring: slot states (ring_cap u32); its
+    uint64_t seq_cap = 0;                //   4-sets use d_jobs with ring_cap entries
+    uint64_t ring_cap = 1ull << 26;
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
     // tuning (ps4_autotune / ps4_set_tuning)
     uint32_t gen_ctas = 2, ext_ctas = 3;     // resident CTAs per SM of the tile kernel / the engine
@@ -135,7 +140,7 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     if (!c) return;
     cudaFree(c->d_spfq); cudaFree(c->d_ndiv); cudaFree(c->d_items); cudaFree(c->d_counters);
     cudaFree(c->d_hits); cudaFree(c->d_exts); cudaFree(c->d_sixes); cudaFree(c->d_quads);
-    cudaFree(c->d_scratch); cudaFree(c->d_status); cudaFree(c->d_jobs); cudaFree(c->d_raw);
+    cudaFree(c->d_scratch); cudaFree(c->d_status); cudaFree(c->d_jobs); cudaFree(c->d_raw); cudaFree(c->d_seq);
     cudaFree(c->d_tri_in); cudaFree(c->d_tri_state); cudaFree(c->d_tri_out); cudaFree(c->d_tri_cnt);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_segs) cudaFreeHost(c->h_segs);
@@ -311,8 +316,10 @@ static void key_add(std::string &k, const T &v) {
 static int enqueue_items(ps4_ctx *c) {
     PendingSearch &p = c->pend;
     const uint32_t n_items = (uint32_t)p.items.size();
-    const unsigned TL = c->tile_log2;
-    const int kernel = c->fused_fallback ? (int)PS4_KERNEL_FUSED : (int)c->cfg.kernel;
+    int kernel = c->fused_fallback ? (int)PS4_KERNEL_FUSED : (int)c->cfg.kernel;
+    if (kernel == PS4_KERNEL_PERSIST && c->persist_fallback) kernel = PS4_KERNEL_BATCHED;
+    const bool persist = kernel == PS4_KERNEL_PERSIST;
+    const unsigned TL = persist ? 13u : c->tile_log2;      // the persistent kernel's tiles are 2^13 S
     if (kernel == PS4_KERNEL_BATCHED) {          // queue: the call's expected 4-sets, 2^20 .. jobs_cap_max
         double need = 0;
         for (uint32_t i = 0; i < n_items; i++)
@@ -324,6 +331,21 @@ static int enqueue_items(ps4_ctx *c) {
     std::vector<uint64_t> batch_tiles;
     if (kernel == PS4_KERNEL_BATCHED) {
         plan_batches(c, p.items, TL, segs, batch_start, batch_tiles);
+    } else if (persist) {
+        // every item in one launch, ordered by estimated cost per tile (the tiles are taken from
+        // the last one down, so the costliest start first and narrow ones fill the tail)
+        segs = p.items;
+        std::stable_sort(segs.begin(), segs.end(), [](const Item &x, const Item &y) {
+            if (x.hi != y.hi) return x.hi < y.hi;
+            return x.hi - x.lo < y.hi - y.lo;
+        });
+        uint64_t tiles = 0;
+        for (auto &sg : segs) {
+            sg.tile_base = tiles;
+            tiles += (sg.hi - sg.lo + (1ull << TL) - 1) >> TL;
+        }
+        batch_start.push_back(0);
+        batch_tiles.push_back(tiles);
     } else {
         uint64_t tiles = 0;
         for (uint32_t i = 0; i < n_items; i++) {
@@ -356,6 +378,16 @@ static int enqueue_items(ps4_ctx *c) {
     if (kernel == PS4_KERNEL_BATCHED &&
         c->raw_words < (uint64_t)c->num_sms * c->gen_ctas * SUPER_K * RAW_PER_TILE)
         if (grow(c, c->d_raw, c->raw_words, (uint64_t)c->num_sms * 2 * SUPER_K * RAW_PER_TILE)) return PS4_ERR_CUDA;
+    const int g_persist = c->num_sms * persist_ctas_per_sm();
+    const uint32_t raw_cap_persist = RAW_PER_TILE / 2;           // 2^13-S tiles: half the representations
+    if (persist) {
+        if (c->d_jobs_words < 6 * c->ring_cap && grow(c, c->d_jobs, c->d_jobs_words, 6 * c->ring_cap))
+            return PS4_ERR_CUDA;
+        if (grow(c, c->d_seq, c->seq_cap, c->ring_cap)) return PS4_ERR_CUDA;
+        if (c->raw_words < (uint64_t)g_persist * SUPER_K * raw_cap_persist &&
+            grow(c, c->d_raw, c->raw_words, (uint64_t)g_persist * SUPER_K * raw_cap_persist))
+            return PS4_ERR_CUDA;
+    }
     const uint32_t stage_cap = stage_cap_for(TL, c->cfg.cap_reps);
     int grid = c->num_sms * (c->cfg.ctas_per_sm ? (int)c->cfg.ctas_per_sm : 1);
     if ((uint64_t)grid > tiles_total) grid = (int)std::max<uint64_t>(tiles_total, 1);
@@ -380,6 +412,16 @@ static int enqueue_items(ps4_ctx *c) {
     a.jobs = c->d_jobs;
     a.jobs_cap = c->jobs_cap;
     if (kernel == PS4_KERNEL_BATCHED) { a.raw = c->d_raw; a.raw_cap = RAW_PER_TILE; }
+    if (persist) {
+        a.jobs_cap = c->ring_cap;
+        a.seq = c->d_seq;
+        a.ring_mask = c->ring_cap - 1;
+        a.ring_fast = 2ull * (uint64_t)g_persist * PBS;          // > every warp claiming 32 at once
+        a.ring_high = 32ull * (uint64_t)g_persist * PBS;         // ~1 ms of engine work at full rate
+        a.ring_low = 4ull * (uint64_t)g_persist * PBS;
+        a.raw = c->d_raw;
+        a.raw_cap = raw_cap_persist;
+    }
     const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
     const int g_gen = c->num_sms * (int)c->gen_ctas, g_ext = c->num_sms * (int)c->ext_ctas;
 
@@ -387,7 +429,8 @@ static int enqueue_items(ps4_ctx *c) {
     // graph is kept and replayed while the next call is the same (items, sizes, buffers).
     const bool graph = !c->cfg.time_kernels &&
                        (c->cfg.use_graph == PS4_GRAPH_ALWAYS ||
-                        (c->cfg.use_graph == PS4_GRAPH_AUTO && kernel == PS4_KERNEL_BATCHED && batch_start.size() >= 2));
+                        (c->cfg.use_graph == PS4_GRAPH_AUTO &&
+                         ((kernel == PS4_KERNEL_BATCHED && batch_start.size() >= 2) || persist)));
     const bool timed = c->cfg.time_kernels && kernel == PS4_KERNEL_BATCHED;
     c->kev_used = 0;
     if (timed) {                                  // 4 events per batch: gen start/end, ext start/end
@@ -444,6 +487,11 @@ static int enqueue_items(ps4_ctx *c) {
                 }
                 if (timed) c->kev_used = 4 * (b + 1);
             }
+        } else if (e == cudaSuccess && persist && tiles_total > 0) {
+            a.items = c->d_items; a.n_items = (uint32_t)segs.size(); a.n_tiles = tiles_total;
+            e = (cudaError_t)launch_ring_init(c->d_seq, c->ring_cap, c->stream);
+            if (e == cudaSuccess) e = (cudaError_t)launch_persist(a, g_persist, c->stream);
+            c->last_launches += 2;
         } else if (e == cudaSuccess && tiles_total > 0) {
             a.items = c->d_items; a.n_items = (uint32_t)segs.size(); a.n_tiles = tiles_total;
             a.scratch = c->d_scratch; a.stage_cap = stage_cap;
@@ -484,6 +532,7 @@ static int begin_items(ps4_ctx *c, const uint64_t *lo, const uint64_t *hi, uint3
     PendingSearch &p = c->pend;
     p.items.assign(n_items, Item{});
     c->fused_fallback = false;
+    c->persist_fallback = false;
     c->last_launches = 0;
     c->last_ms = 0.0;
     c->h2d_bytes = c->d2h_bytes = 0;
@@ -551,7 +600,16 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
             if (c->batch_div < (1u << 16)) { c->batch_div *= 2; continue; }
             return set_err(c, PS4_ERR_CUDA, "job queue overflow persists near S=%llu", errS);
         }
-        if (code == E_EXTLIST && c->cfg.kernel == PS4_KERNEL_BATCHED && !c->fused_fallback) {
+        if ((code == E_TIMEOUT || code == E_TILE) && c->cfg.kernel == PS4_KERNEL_PERSIST && !c->persist_fallback &&
+            !c->fused_fallback) {
+            c->persist_fallback = true;          // the two-kernel pipeline: no waits, smaller tiles on E_TILE
+            continue;
+        }
+        if (code == E_TIMEOUT)
+            return set_err(c, PS4_ERR_TIMEOUT, "a bounded device wait gave up (wait %llu); the call did not complete",
+                           errS);
+        if (code == E_EXTLIST && (c->cfg.kernel == PS4_KERNEL_BATCHED || c->cfg.kernel == PS4_KERNEL_PERSIST) &&
+            !c->fused_fallback) {
             c->fused_fallback = true;            // more extensions in one engine round than its list holds: fused kernel
             continue;
         }
@@ -693,6 +751,46 @@ extern "C" int ps4_plan_shards(uint64_t lo, uint64_t hi, uint32_t n, uint64_t *b
     }
     bounds[n] = hi;
     return PS4_OK;
+}
+
+// ---- self-check of the persistent kernel's bounded wait ----
+
+extern "C" int ps4_check_ring_wait(int device, uint64_t *waited_ns) {
+    if (waited_ns) *waited_ns = 0;
+    int prev = 0;
+    if (cudaGetDevice(&prev) != cudaSuccess || cudaSetDevice(device) != cudaSuccess) return PS4_ERR_CUDA;
+    Status *d_st = nullptr;
+    uint32_t *d_seq = nullptr;
+    unsigned long long *d_out = nullptr;
+    cudaError_t e = cudaMalloc((void **)&d_st, sizeof(Status));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_seq, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc((void **)&d_out, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(d_st, 0, sizeof(Status));
+    if (e == cudaSuccess) e = cudaMemset(d_seq, 0, sizeof(uint32_t));     // position 0 never published
+    int rc = PS4_ERR_CUDA;
+    if (e == cudaSuccess) {
+        SearchArgs a;
+        memset(&a, 0, sizeof a);
+        a.status = d_st;
+        a.seq = d_seq;
+        a.ring_mask = 0;
+        a.jobs_cap = 1;
+        a.n_tiles = 1;                                  // a tile still to come: the wait cannot end early
+        e = (cudaError_t)launch_ring_wait_probe(a, d_out, nullptr);
+        unsigned long long out[2] = {0, 0};
+        Status st;
+        if (e == cudaSuccess) e = cudaMemcpy(out, d_out, sizeof out, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) e = cudaMemcpy(&st, d_st, sizeof st, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) {
+            if (waited_ns) *waited_ns = out[1];
+            rc = (out[0] == 0 && (st.err & 0xFF) == E_TIMEOUT && (st.err >> 8) == 1) ? PS4_ERR_TIMEOUT : PS4_OK;
+        }
+    }
+    cudaFree(d_st);
+    cudaFree(d_seq);
+    cudaFree(d_out);
+    if (prev != device) cudaSetDevice(prev);
+    return rc;
 }
 
 // ---- tuning ----

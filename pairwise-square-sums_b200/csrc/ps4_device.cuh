@@ -282,9 +282,11 @@ __device__ inline void extend_quad(const SearchArgs &a, const uint32_t r[6], con
 
 // ------------------------------------------------------------------ block helpers
 
-// exclusive block scan of three u32 values; returns totals in tot[3]
+// exclusive block scan of three u32 values over NT threads; returns totals in tot[3]
+template <int NT = BS>
 __device__ __forceinline__ void block_scan3(uint32_t x0, uint32_t x1, uint32_t x2, uint32_t &e0, uint32_t &e1,
-                                            uint32_t &e2, uint32_t tot[3], uint32_t *wsum /* 3*NWARP */) {
+                                            uint32_t &e2, uint32_t tot[3], uint32_t *wsum /* 3*NWARP; 3*NT/32 used */) {
+    constexpr int NW = NT / 32;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     uint32_t i0 = x0, i1 = x1, i2 = x2;
 #pragma unroll
@@ -293,24 +295,24 @@ __device__ __forceinline__ void block_scan3(uint32_t x0, uint32_t x1, uint32_t x
                  y2 = __shfl_up_sync(0xffffffffu, i2, o);
         if (lane >= o) { i0 += y0; i1 += y1; i2 += y2; }
     }
-    if (lane == 31) { wsum[wid] = i0; wsum[NWARP + wid] = i1; wsum[2 * NWARP + wid] = i2; }
+    if (lane == 31) { wsum[wid] = i0; wsum[NW + wid] = i1; wsum[2 * NW + wid] = i2; }
     __syncthreads();
     if (wid == 0) {
-        uint32_t s0 = lane < NWARP ? wsum[lane] : 0, s1 = lane < NWARP ? wsum[NWARP + lane] : 0,
-                 s2 = lane < NWARP ? wsum[2 * NWARP + lane] : 0;
+        uint32_t s0 = lane < NW ? wsum[lane] : 0, s1 = lane < NW ? wsum[NW + lane] : 0,
+                 s2 = lane < NW ? wsum[2 * NW + lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y0 = __shfl_up_sync(0xffffffffu, s0, o), y1 = __shfl_up_sync(0xffffffffu, s1, o),
                      y2 = __shfl_up_sync(0xffffffffu, s2, o);
             if (lane >= o) { s0 += y0; s1 += y1; s2 += y2; }
         }
-        if (lane < NWARP) { wsum[lane] = s0; wsum[NWARP + lane] = s1; wsum[2 * NWARP + lane] = s2; }
+        if (lane < NW) { wsum[lane] = s0; wsum[NW + lane] = s1; wsum[2 * NW + lane] = s2; }
     }
     __syncthreads();
-    const uint32_t b0 = wid ? wsum[wid - 1] : 0, b1 = wid ? wsum[NWARP + wid - 1] : 0,
-                   b2 = wid ? wsum[2 * NWARP + wid - 1] : 0;
+    const uint32_t b0 = wid ? wsum[wid - 1] : 0, b1 = wid ? wsum[NW + wid - 1] : 0,
+                   b2 = wid ? wsum[2 * NW + wid - 1] : 0;
     e0 = b0 + i0 - x0; e1 = b1 + i1 - x1; e2 = b2 + i2 - x2;
-    tot[0] = wsum[NWARP - 1]; tot[1] = wsum[2 * NWARP - 1]; tot[2] = wsum[3 * NWARP - 1];
+    tot[0] = wsum[NW - 1]; tot[1] = wsum[2 * NW - 1]; tot[2] = wsum[3 * NW - 1];
     __syncthreads();
 }
 
@@ -385,7 +387,7 @@ __device__ __forceinline__ uint32_t isqrt_lt2p46(uint64_t x) {
 // P1 / P3: scan every representation S = p^2 + q^2, 1 <= p <= q, S in [S0, S0+n).
 // q-major: q runs over [ceil(sqrt(S0/2)), isqrt(S1-2)] (strided over the threads), p from
 // ceil(sqrt(S0-q^2)) by a float estimate with exact integer correction (S < 2^44).
-template <bool FILL>
+template <bool FILL, int NT = BS>
 __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t *cnt32, uint32_t *rep_p,
                                               uint32_t *rep_q) {
     const uint64_t S1 = S0 + n;
@@ -393,7 +395,7 @@ __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t 
     if (qmin < 1) qmin = 1;
     const uint32_t qmax = S1 >= 2 ? (uint32_t)isqrt64(S1 - 2) : 0;
     uint32_t found = 0;
-    for (uint32_t q = qmin + threadIdx.x; q <= qmax; q += BS) {
+    for (uint32_t q = qmin + threadIdx.x; q <= qmax; q += NT) {
         const uint64_t q2 = (uint64_t)q * q;
         uint32_t p = 1;
         if (S0 > q2 + 1) {
@@ -422,7 +424,8 @@ __device__ __forceinline__ uint32_t scan_reps(uint64_t S0, uint32_t n, uint32_t 
 // segment, done once: every representation goes to its tile's list (offset in the tile | p << 14 |
 // q << 36; p <= q < 2^22, offset < 2^14), in the slice of the warp that found it (one shared
 // atomic per representation).  Slice counts above `slice` mean the list overflowed; that tile
-// then scans for itself.
+// then scans for itself.  NT threads, NT/32 warp slices per tile.
+template <int NT = BS>
 __device__ __forceinline__ void scan_group(uint64_t SS0, uint64_t SS1, unsigned TLv, uint64_t *lists,
                                            uint32_t list_cap, uint32_t *raw_n, uint32_t slice) {
     uint32_t qmin = (uint32_t)ceil_sqrt64((SS0 + 1) >> 1);
@@ -430,7 +433,7 @@ __device__ __forceinline__ void scan_group(uint64_t SS0, uint64_t SS1, unsigned 
     const uint32_t qmax = SS1 >= 2 ? (uint32_t)isqrt64(SS1 - 2) : 0;
     const int wid = threadIdx.x >> 5;
     const uint32_t wmask = (1u << TLv) - 1u;
-    for (uint32_t q = qmin + threadIdx.x; q <= qmax; q += BS) {
+    for (uint32_t q = qmin + threadIdx.x; q <= qmax; q += NT) {
         const uint64_t q2 = (uint64_t)q * q;
         uint32_t p = 1;
         if (SS0 > q2 + 1) {
@@ -440,7 +443,7 @@ __device__ __forceinline__ void scan_group(uint64_t SS0, uint64_t SS1, unsigned 
         }
         for (uint64_t s = (uint64_t)p * p + q2; p <= q && s < SS1; s += 2 * p + 1, p++) {
             const uint32_t i = (uint32_t)(s - SS0), j = i >> TLv;
-            const uint32_t pos = atomicAdd(&raw_n[j * NWARP + wid], 1u);
+            const uint32_t pos = atomicAdd(&raw_n[j * (NT / 32) + wid], 1u);
             if (pos < slice)
                 lists[(size_t)j * list_cap + (size_t)wid * slice + pos] =
                     (uint64_t)(i & wmask) | ((uint64_t)p << 14) | ((uint64_t)q << 36);
@@ -451,7 +454,7 @@ __device__ __forceinline__ void scan_group(uint64_t SS0, uint64_t SS1, unsigned 
 // P1-P4 for one tile.  Returns false if the tile was abandoned (error raised).  With `list` (the
 // tile's representations from scan_group, list_n[w] entries in warp slice w of `slice`) P1 and
 // P3 read the list; without, they scan.
-template <int TL>
+template <int TL, int NT = BS>
 __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *smem, uint64_t S0, uint32_t n,
                           const uint64_t *list = nullptr, const uint32_t *list_n = nullptr, uint32_t slice = 0) {
     using L = TileLayout<TL>;
@@ -464,21 +467,21 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
     uint32_t *rep_q = (uint32_t *)(smem + L::OFF_REP_Q);
     const int tid = threadIdx.x;
 
-    for (uint32_t i = tid; i < L::W / 2; i += BS) cnt32[i] = 0;
+    for (uint32_t i = tid; i < L::W / 2; i += NT) cnt32[i] = 0;
     __syncthreads();
     // P1: count, from the list or by scanning
     uint32_t found = 0;
     if (list) {
-        for (int w = 0; w < NWARP; w++) {
+        for (int w = 0; w < NT / 32; w++) {
             const uint32_t cw = list_n[w];
-            for (uint32_t o = tid; o < cw; o += BS) {
+            for (uint32_t o = tid; o < cw; o += NT) {
                 const uint32_t i = (uint32_t)list[(size_t)w * slice + o] & 0x3FFFu;
                 atomicAdd(&cnt32[i >> 1], 1u << ((i & 1) * 16));
                 found++;
             }
         }
     } else {
-        found = scan_reps<false>(S0, n, cnt32, rep_p, rep_q);
+        found = scan_reps<false, NT>(S0, n, cnt32, rep_p, rep_q);
     }
     ull f = warp_sum((ull)found);
     if ((tid & 31) == 0 && f) atomicAdd(&ts.cnt[K_PAIRS], f);
@@ -487,7 +490,7 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
     // P2: select S with >= 3 representations and S != 2 (mod 4).  A thread owns SEG consecutive
     // S, i.e. WT counter words, and visits them from a lane-dependent rotation so that the lanes
     // of a warp touch 32 different banks (in plain order they would all hit the same two)
-    constexpr uint32_t SEG = L::W / BS;
+    constexpr uint32_t SEG = L::W / NT;
     constexpr uint32_t WT = SEG / 2;
     static_assert(WT >= 1 && WT <= 32 && (WT & (WT - 1)) == 0, "counter words per thread: a power of two");
     const uint32_t i0 = tid * SEG, w0 = tid * WT;
@@ -513,7 +516,7 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
     }
     if (over) raise_error(a.status, E_CAP_REPS, S0);
     uint32_t bI, bR, bP, tot[3];
-    block_scan3(nI, nR, nP, bI, bR, bP, tot, ts.wsum);
+    block_scan3<NT>(nI, nR, nP, bI, bR, bP, tot, ts.wsum);
     {
         const ull tw = warp_sum(trip);
         const uint32_t km = warp_max(kmax);
@@ -559,9 +562,9 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
     __syncthreads();
     // P3: fill, from the list or by scanning again
     if (list) {
-        for (int w = 0; w < NWARP; w++) {
+        for (int w = 0; w < NT / 32; w++) {
             const uint32_t cw = list_n[w];
-            for (uint32_t o = tid; o < cw; o += BS) {
+            for (uint32_t o = tid; o < cw; o += NT) {
                 const uint64_t e = list[(size_t)w * slice + o];
                 const uint32_t i = (uint32_t)e & 0x3FFFu, wd = i >> 1, sh = (i & 1) * 16;
                 const uint32_t cur = (((volatile uint32_t *)cnt32)[wd] >> sh) & 0xFFFFu;
@@ -572,11 +575,11 @@ __device__ bool tile_reps(const SearchArgs &a, TileShared &ts, unsigned char *sm
             }
         }
     } else {
-        scan_reps<true>(S0, n, cnt32, rep_p, rep_q);
+        scan_reps<true, NT>(S0, n, cnt32, rep_p, rep_q);
     }
     __syncthreads();
     // P4: each list ascending in p
-    for (uint32_t s = tid; s < ts.n_is; s += BS) {
+    for (uint32_t s = tid; s < ts.n_is; s += NT) {
         const uint32_t st = is_start[s], k = is_k[s];
         for (uint32_t x = st + 1; x < st + k; x++) {
             const uint32_t kp = rep_p[x], kq = rep_q[x];

@@ -39,23 +39,126 @@ __device__ __forceinline__ void put_job(uint32_t *jobs, uint64_t cap, uint64_t j
     jobs[5 * cap + j] = r[5];
 }
 
+// COH: the queue is a ring whose slots are rewritten while the kernel runs, so its words are read
+// through L2 (coherent), not the read-only path that may hold a slot's previous 4-set.
+template <bool COH = false>
+__device__ __forceinline__ uint32_t ld_job(const uint32_t *p) { return COH ? __ldcg(p) : __ldg(p); }
+
+template <bool COH = false>
 __device__ __forceinline__ void get_job(const uint32_t *jobs, uint64_t cap, uint64_t j, uint32_t r[6],
                                         uint32_t &item) {
-    const uint32_t w1 = __ldg(&jobs[cap + j]), w2 = __ldg(&jobs[2 * cap + j]);
-    r[0] = __ldg(&jobs[j]);
+    const uint32_t w1 = ld_job<COH>(&jobs[cap + j]), w2 = ld_job<COH>(&jobs[2 * cap + j]);
+    r[0] = ld_job<COH>(&jobs[j]);
     r[1] = w1 & 0x3FFFFFu;
     r[2] = w2 & 0x3FFFFFu;
-    r[3] = __ldg(&jobs[3 * cap + j]);
-    r[4] = __ldg(&jobs[4 * cap + j]);
-    r[5] = __ldg(&jobs[5 * cap + j]);
+    r[3] = ld_job<COH>(&jobs[3 * cap + j]);
+    r[4] = ld_job<COH>(&jobs[4 * cap + j]);
+    r[5] = ld_job<COH>(&jobs[5 * cap + j]);
     item = (w1 >> 22) | ((w2 >> 22) << 10);
+}
+
+// ================================================================== the persistent kernel's ring
+//
+// Producing CTAs reserve positions (q_tail), wait until each position's slot is free of its
+// previous lap, write the 4-set, and publish it: seq[slot] = pos + 1 after a fence.  Consuming
+// warps claim positions below q_tail (q_head), wait until each is published, and after the 4-set
+// is extended and reported free its slot: seq[slot] = pos + ring size.  Every wait is bounded in
+// time (WAIT_NS); a wait that gives up sets the error word to E_TIMEOUT (with which wait in the S
+// field: 1 published, 2 slot free, 3 ring room, 4 idle) and the kernel ends, the host re-running
+// the call on the two-kernel pipeline.
+
+__device__ __forceinline__ uint64_t gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ uint32_t ld_vol(const uint32_t *p) { return *(const volatile uint32_t *)p; }
+__device__ __forceinline__ ull ld_vol(const ull *p) { return *(const volatile ull *)p; }
+
+// Tracks one wait's elapsed time: true once it has lasted WAIT_NS (and records the timeout).
+struct WaitClock {
+    uint64_t t0 = 0;
+    __device__ __forceinline__ bool expired(const SearchArgs &a, unsigned which) {
+        const uint64_t t = gtimer();
+        if (!t0) { t0 = t; return false; }
+        if (t - t0 <= WAIT_NS) return false;
+        raise_error(a.status, E_TIMEOUT, which);
+        return true;
+    }
+};
+
+// A producer's slot: wait until it is free for position pos.  False if the call stopped.
+__device__ __noinline__ bool ring_wait_free(const SearchArgs &a, uint64_t pos) {
+    const uint32_t *f = a.seq + (pos & a.ring_mask);
+    WaitClock wc;
+    for (uint32_t k = 0;; k++) {
+        if (ld_vol(f) == (uint32_t)pos) return true;
+        if ((k & 15) == 15 && (ld_vol(&a.status->err) != 0ull || wc.expired(a, 2))) return false;
+        __nanosleep(64);
+    }
+}
+
+// A consumer's claimed position: wait until its 4-set is published.  False if the call stopped,
+// or if the position will never be written (every tile is produced and the position lies past
+// the last reserved one: a claim that overtook the reservations, see ring_claim).
+__device__ __noinline__ bool ring_wait_ready(const SearchArgs &a, uint64_t pos) {
+    const uint32_t *f = a.seq + (pos & a.ring_mask);
+    WaitClock wc;
+    for (uint32_t k = 0;; k++) {
+        if (ld_vol(f) == (uint32_t)(pos + 1)) {
+            __threadfence();                       // the 4-set's words after its flag
+            return true;
+        }
+        if ((k & 15) == 15) {
+            if (ld_vol(&a.status->err) != 0ull) return false;
+            if (ld_vol(&a.status->q_produced) >= a.n_tiles && pos >= ld_vol(&a.status->q_tail)) return false;
+            if (wc.expired(a, 1)) return false;
+        }
+        __nanosleep(32);
+    }
+}
+
+__device__ __forceinline__ void ring_release(const SearchArgs &a, uint64_t pos) {
+    __threadfence();                               // every read of the slot before it is handed back
+    *(volatile uint32_t *)&a.seq[pos & a.ring_mask] = (uint32_t)(pos + a.ring_mask + 1);
+}
+
+// Claim up to n positions below q_tail (one lane of a warp).  While tiles are left, fewer than
+// ring_low queued 4-sets are left for later (the warp stops consuming, its CTA turns to tiles).
+// While at least ring_fast reserved positions are unclaimed, an add cannot overtake the
+// reservations (every warp of the grid claiming at once takes fewer), so it is used; closer to
+// q_tail a compare-and-swap claims only what is reserved.  *got receives the count, the first
+// position is returned.
+__device__ __forceinline__ uint64_t ring_claim(const SearchArgs &a, uint32_t n, uint32_t *got) {
+    ull *head = &a.status->q_head;
+    ull h = ld_vol(head);
+    const ull t = ld_vol(&a.status->q_tail);
+    *got = 0;
+    if ((long long)(t - h) <= 0) return 0;
+    if (t - h < a.ring_low && ld_vol(&a.status->tile_next) < a.n_tiles) return 0;
+    if (t - h >= a.ring_fast) {
+        *got = n;
+        return atomicAdd(head, (ull)n);
+    }
+    for (int k = 0; k < 16; k++) {
+        const ull tt = ld_vol(&a.status->q_tail);
+        if ((long long)(tt - h) <= 0) break;
+        const ull take = tt - h < n ? tt - h : n;
+        const ull prev = atomicCAS(head, h, h + take);
+        if (prev == h) {
+            *got = (uint32_t)take;
+            return h;
+        }
+        h = prev;
+    }
+    return 0;
 }
 
 // ================================================================== gen_jobs
 
 // The 4-sets of representation pair gidx of the tile (P5), pair given as list s and (x, y).
 // Counts them; with WRITE also builds, checks, dumps and (when `store`) queues them at out, ...
-template <bool WRITE>
+template <bool WRITE, bool RING = false>
 __device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t st, uint32_t k, uint64_t S,
                                                uint32_t x, uint32_t y, const uint32_t *rep_p,
                                                const uint32_t *rep_q, uint32_t item, uint64_t out, bool store) {
@@ -85,7 +188,13 @@ __device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t st,
                     if (!quad_roots_ok(v, r)) record_verify_failure(a, S, v);
                 }
                 if (a.flags & PS4_F_DUMP4) dump_quad(a, r);
-                if (store) put_job(a.jobs, a.jobs_cap, out + n, r, item);
+                if (store) {
+                    if (!RING) {
+                        put_job(a.jobs, a.jobs_cap, out + n, r, item);
+                    } else if (ring_wait_free(a, out + n)) {
+                        put_job(a.jobs, a.jobs_cap, (out + n) & a.ring_mask, r, item);
+                    }
+                }
             }
             n++;
         }
@@ -96,7 +205,7 @@ __device__ __forceinline__ uint32_t pair_quads(const SearchArgs &a, uint32_t st,
 // A lane's share of P5: the pairs g = gw + lane, gw + lane + 32, ... below ge of its warp's
 // contiguous block.  Neighbouring lanes take neighbouring pairs (mostly the same S), and each
 // lane finds its pair's S by one binary search, then by stepping forward.
-template <bool WRITE>
+template <bool WRITE, bool RING = false>
 __device__ __forceinline__ uint32_t lane_pairs(const SearchArgs &a, uint32_t gw, uint32_t ge, int lane, uint32_t nI,
                                                const uint16_t *is_off, const uint16_t *is_k,
                                                const uint16_t *is_start, const uint32_t *is_pbase,
@@ -114,9 +223,119 @@ __device__ __forceinline__ uint32_t lane_pairs(const SearchArgs &a, uint32_t gw,
         while (lo + 1 < nI && is_pbase[lo + 1] <= g) lo++;
         uint32_t x, y;
         decode_pair(g - is_pbase[lo], x, y);
-        n += pair_quads<WRITE>(a, is_start[lo], is_k[lo], S0 + is_off[lo], x, y, rep_p, rep_q, item, out + n, store);
+        n += pair_quads<WRITE, RING>(a, is_start[lo], is_k[lo], S0 + is_off[lo], x, y, rep_p, rep_q, item, out + n,
+                                     store);
     }
     return n;
+}
+
+// One claimed group of tiles, the last-but-c0 SUPER_K tiles of the launch (tiles are taken from
+// the last one down, costliest first): per segment of the group one scan for all its tiles (from
+// S = SUPER_MIN_S up), then per tile P1-P4, the count pass, one reservation for the tile's
+// 4-sets, the write pass.  NT threads.  RING: the 4-sets go to the persistent kernel's ring and
+// each lane publishes its contiguous run after a fence.  Returns the number of tiles.
+template <int TL, int NT, bool RING>
+__device__ uint32_t produce_group(const SearchArgs &a, TileShared &ts, unsigned char *smem, uint64_t c0,
+                                  uint64_t *lists, uint32_t *raw_n, uint32_t slice, unsigned long long &s_base,
+                                  int &s_store) {
+    using L = TileLayout<TL>;
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x;
+    const bool noext = (a.flags & PS4_F_NOEXT) != 0;
+    const bool need_write_pass = !noext || (a.flags & (PS4_F_DUMP4 | PS4_F_VERIFY));
+    const uint64_t cn = min((uint64_t)SUPER_K, a.n_tiles - c0);
+    uint64_t ti = a.n_tiles - c0 - cn;
+    const uint64_t ti_end = a.n_tiles - c0;
+    while (ti < ti_end) {
+        // a group: the claimed tiles of one segment, one scan for all of them
+        uint32_t lo = 0, hi = a.n_items;
+        while (hi - lo > 1) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (a.items[mid].tile_base <= ti) lo = mid; else hi = mid;
+        }
+        const Item it = a.items[lo];
+        const uint64_t seg_tiles = (it.hi - it.lo + (1ull << TL) - 1) >> TL;
+        const uint64_t g_end = min(ti_end, it.tile_base + seg_tiles);
+        const uint32_t ng = (uint32_t)(g_end - ti);
+        const uint64_t SA = it.lo + ((ti - it.tile_base) << TL);
+        const uint64_t SB = min(it.hi, SA + ((uint64_t)ng << TL));
+        const uint32_t item = it.id;
+        const bool grouped = lists != nullptr && SA >= SUPER_MIN_S;
+        if (grouped) {
+            if (tid < SUPER_K * NW) raw_n[tid] = 0;
+            __syncthreads();
+            scan_group<NT>(SA, SB, TL, lists, a.raw_cap, raw_n, slice);
+            __syncthreads();
+        }
+        for (uint32_t j = 0; j < ng; j++) {
+            tile_reset(ts);
+            __syncthreads();
+            const uint64_t S0 = SA + ((uint64_t)j << TL);
+            const uint32_t n = (uint32_t)min((uint64_t)L::W, SB - S0);
+            bool use_list = grouped;
+            for (int w = 0; w < NW; w++) use_list = use_list && raw_n[j * NW + w] <= slice;
+            if (!tile_reps<TL, NT>(a, ts, smem, S0, n, use_list ? lists + (size_t)j * a.raw_cap : nullptr,
+                                   &raw_n[j * NW], slice)) { __syncthreads(); continue; }
+            const uint16_t *is_off = (const uint16_t *)(smem + L::OFF_IS_OFF);
+            const uint16_t *is_k = (const uint16_t *)(smem + L::OFF_IS_K);
+            const uint16_t *is_start = (const uint16_t *)(smem + L::OFF_IS_START);
+            const uint32_t *is_pbase = (const uint32_t *)(smem + L::OFF_IS_PBASE);
+            const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
+            const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
+            const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
+            // count pass, one reservation for the tile, write pass in the same order
+            // each warp a contiguous block of pairs (whole multiples of 32)
+            const int lane = tid & 31, wid = tid >> 5;
+            const uint32_t blk = ((nPairs + NW * 32 - 1) / (NW * 32)) * 32;
+            const uint32_t gw = (uint32_t)wid * blk, ge = min(nPairs, gw + blk);
+            uint32_t mine = lane_pairs<false>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0,
+                                              item, 0, false);
+            uint32_t off, d1, d2, tot[3];
+            block_scan3<NT>(mine, 0u, 0u, off, d1, d2, tot, ts.wsum);
+            if (tid == 0) {
+                ts.cnt[K_SETS4] += tot[0];
+                s_base = 0;
+                s_store = 0;
+                if (!noext && tot[0]) {
+                    if (RING) {
+                        // room: the ring holds the reserved-but-unfinished 4-sets plus this tile's
+                        WaitClock wc;
+                        bool ok = true;
+                        while (ld_vol(&a.status->q_tail) + tot[0] - ld_vol(&a.status->q_freed) > a.jobs_cap) {
+                            if (ld_vol(&a.status->err) != 0ull || wc.expired(a, 3)) { ok = false; break; }
+                            __nanosleep(256);
+                        }
+                        if (ok) {
+                            s_base = atomicAdd(&a.status->q_tail, (ull)tot[0]);
+                            s_store = 1;
+                        }
+                    } else {
+                        s_base = atomicAdd(&a.status->n_jobs, (ull)tot[0]);
+                        if (s_base + tot[0] <= a.jobs_cap) s_store = 1;
+                        else raise_capacity(a.status, E_QUEUE, 5, s_base + tot[0], a.jobs_cap, S0);
+                    }
+                }
+            }
+            __syncthreads();
+            if (need_write_pass) {
+                const bool store = s_store != 0;
+                lane_pairs<true, RING>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item,
+                                       s_base + off, store);
+                if (RING && store && mine) {       // publish this lane's run [s_base+off, +mine)
+                    __threadfence();
+                    for (uint32_t i = 0; i < mine; i++) {
+                        const uint64_t pos = s_base + off + i;
+                        *(volatile uint32_t *)&a.seq[pos & a.ring_mask] = (uint32_t)(pos + 1);
+                    }
+                }
+            }
+            __syncthreads();
+            tile_flush_counters(a, ts, item);
+            __syncthreads();
+        }
+        ti = g_end;
+    }
+    return (uint32_t)cn;
 }
 
 template <int TL>
@@ -126,10 +345,8 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
     __shared__ TileShared ts;
     __shared__ unsigned long long s_base;
     __shared__ int s_store;
-    const int tid = threadIdx.x;
-    const bool noext = (a.flags & PS4_F_NOEXT) != 0;
-    const bool need_write_pass = !noext || (a.flags & (PS4_F_DUMP4 | PS4_F_VERIFY));
     __shared__ unsigned long long s_claim;
+    const int tid = threadIdx.x;
     uint64_t *lists = a.raw ? a.raw + (size_t)blockIdx.x * SUPER_K * a.raw_cap : nullptr;
     // per tile of a group and warp: representations appended to the tile's list; in the tile
     // layout's extension-list area, which this kernel does not use otherwise
@@ -146,77 +363,7 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
         const bool stop = c0 >= a.n_tiles || ts.skip;
         __syncthreads();                                                 // s_claim read by all
         if (stop) break;                                                 // block-uniform
-        const uint64_t cn = min((uint64_t)SUPER_K, a.n_tiles - c0);
-        uint64_t ti = a.n_tiles - c0 - cn;
-        const uint64_t ti_end = a.n_tiles - c0;
-        while (ti < ti_end) {
-            // a group: the claimed tiles of one segment, one scan for all of them
-            uint32_t lo = 0, hi = a.n_items;
-            while (hi - lo > 1) {
-                const uint32_t mid = (lo + hi) >> 1;
-                if (a.items[mid].tile_base <= ti) lo = mid; else hi = mid;
-            }
-            const Item it = a.items[lo];
-            const uint64_t seg_tiles = (it.hi - it.lo + (1ull << TL) - 1) >> TL;
-            const uint64_t g_end = min(ti_end, it.tile_base + seg_tiles);
-            const uint32_t ng = (uint32_t)(g_end - ti);
-            const uint64_t SA = it.lo + ((ti - it.tile_base) << TL);
-            const uint64_t SB = min(it.hi, SA + ((uint64_t)ng << TL));
-            const uint32_t item = it.id;
-            const bool grouped = lists != nullptr && SA >= SUPER_MIN_S;
-            if (grouped) {
-                if (tid < SUPER_K * NWARP) raw_n[tid] = 0;
-                __syncthreads();
-                scan_group(SA, SB, TL, lists, a.raw_cap, raw_n, slice);
-                __syncthreads();
-            }
-            for (uint32_t j = 0; j < ng; j++) {
-                tile_reset(ts);
-                __syncthreads();
-                const uint64_t S0 = SA + ((uint64_t)j << TL);
-                const uint32_t n = (uint32_t)min((uint64_t)L::W, SB - S0);
-                bool use_list = grouped;
-                for (int w = 0; w < NWARP; w++) use_list = use_list && raw_n[j * NWARP + w] <= slice;
-                if (!tile_reps<TL>(a, ts, smem, S0, n, use_list ? lists + (size_t)j * a.raw_cap : nullptr,
-                                   &raw_n[j * NWARP], slice)) { __syncthreads(); continue; }
-                const uint16_t *is_off = (const uint16_t *)(smem + L::OFF_IS_OFF);
-                const uint16_t *is_k = (const uint16_t *)(smem + L::OFF_IS_K);
-                const uint16_t *is_start = (const uint16_t *)(smem + L::OFF_IS_START);
-                const uint32_t *is_pbase = (const uint32_t *)(smem + L::OFF_IS_PBASE);
-                const uint32_t *rep_p = (const uint32_t *)(smem + L::OFF_REP_P);
-                const uint32_t *rep_q = (const uint32_t *)(smem + L::OFF_REP_Q);
-                const uint32_t nI = ts.n_is, nPairs = ts.n_pairs;
-                // count pass, one reservation for the tile, write pass in the same order
-                // each warp a contiguous block of pairs (whole multiples of 32)
-                const int lane = tid & 31, wid = tid >> 5;
-                const uint32_t blk = ((nPairs + NWARP * 32 - 1) / (NWARP * 32)) * 32;
-                const uint32_t gw = (uint32_t)wid * blk, ge = min(nPairs, gw + blk);
-                uint32_t mine = lane_pairs<false>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0,
-                                                  item, 0, false);
-                uint32_t off, d1, d2, tot[3];
-                block_scan3(mine, 0u, 0u, off, d1, d2, tot, ts.wsum);
-                if (tid == 0) {
-                    ts.cnt[K_SETS4] += tot[0];
-                    s_base = 0;
-                    s_store = 0;
-                    if (!noext && tot[0]) {
-                        s_base = atomicAdd(&a.status->n_jobs, (ull)tot[0]);
-                        if (s_base + tot[0] <= a.jobs_cap) s_store = 1;
-                        else raise_capacity(a.status, E_QUEUE, 5, s_base + tot[0], a.jobs_cap, S0);
-                    }
-                }
-                __syncthreads();
-                if (need_write_pass) {
-                    const bool store = s_store != 0;
-                    lane_pairs<true>(a, gw, ge, lane, nI, is_off, is_k, is_start, is_pbase, rep_p, rep_q, S0, item,
-                                     s_base + off, store);
-                }
-                __syncthreads();
-                tile_flush_counters(a, ts, item);
-                __syncthreads();
-            }
-            ti = g_end;
-        }
+        produce_group<TL, BS, false>(a, ts, smem, c0, lists, raw_n, slice, s_base, s_store);
     }
 }
 
@@ -326,6 +473,7 @@ struct LaneCounters {
 
 // Report the extensions of one warp round: group them per 4-set, emit hit / ext / six
 // records and the counters sets5 / multi / sets6 / hist5 / max_extensions (s4.c:243-277).
+template <bool COH>
 static __device__ void report_warp_exts(const SearchArgs &a, ExtEntry *el, uint32_t n) {
     for (uint32_t x = 1; x < n; x++) {
         ExtEntry k = el[x];
@@ -341,7 +489,7 @@ static __device__ void report_warp_exts(const SearchArgs &a, ExtEntry *el, uint3
         while (g1 < n && el[g1].qid == el[g0].qid) g1++;
         const uint32_t ne = g1 - g0;
         uint32_t roots[6], item;                              // the 4-set and its item, from the queue
-        get_job(a.jobs, a.jobs_cap, el[g0].qid, roots, item);
+        get_job<COH>(a.jobs, a.jobs_cap, el[g0].qid, roots, item);
         ull *cnt = a.counters + (size_t)item * K_SLOTS;
         uint64_t v[4], S;
         quad_values(roots, v, S);
@@ -463,9 +611,10 @@ __device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, ui
     return np;
 }
 
+template <bool COH>
 __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJob &J, uint32_t (*fp)[32],
                                           int lane) {
-    get_job(a.jobs, a.jobs_cap, j, J.r, J.item);
+    get_job<COH>(a.jobs, a.jobs_cap, j, J.r, J.item);
     quad_values(J.r, J.v, J.S);
     uint32_t best;
     choose_pair(J.v, J.r, a.ndiv, J.bi, J.bj, J.bk, best);
@@ -560,19 +709,22 @@ __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, 
     }
 }
 
-__global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
-    extern __shared__ __align__(16) unsigned char esmem[];
-    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    WarpArea *w = (WarpArea *)(esmem + (size_t)wid * sizeof(WarpArea));
+// The engine loop of one warp.  Linear (RING false): the batch's queue [0, njobs), filled before
+// the launch; the loop ends when it is drained.  RING: the persistent kernel's ring; positions are
+// claimed below q_tail and waited for until published, each finished 4-set's slot is handed back
+// after the round's report, and the loop ends when a claim finds the ring empty and no lane holds
+// a 4-set.  Returns whether the warp took any 4-set.
+template <bool RING>
+__device__ __forceinline__ bool engine_loop(const SearchArgs &a, WarpArea *w, int lane, uint64_t njobs) {
     const unsigned FULL = 0xffffffffu;
-    const uint64_t njobs = min(*(volatile ull *)&a.status->n_jobs, (ull)a.jobs_cap);
     if (lane == 0) w->n_ext = 0;
     w->jsq[lane] = 0;
     __syncwarp();
     LaneCounters cnt;
     LaneJob J;
-    bool pending = false, old = false, drained = false;
+    bool pending = false, old = false, drained = false, rel = false, took = false;
     uint32_t myjob = 0;
+    uint64_t mypos = 0;
 
     // Rolling rounds: before each round every lane without a 4-set takes the next one from the
     // queue (phase A), so every round runs with a full warp of 4-sets; a lane whose divisor
@@ -581,23 +733,45 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
         if (!drained) {
             const bool need = !pending;
             const unsigned m = __ballot_sync(FULL, need);
-            uint32_t base = 0;
+            uint64_t base = 0;
+            uint32_t got = 0;
             int stop = 0;
-            if (lane == 0) {
-                if (m) base = atomicAdd(&a.status->ext_next, (uint32_t)__popc(m));
-                stop = *(volatile ull *)&a.status->err != 0ull;
+            if (RING) {
+                if (lane == 0) {
+                    if (m) base = ring_claim(a, (uint32_t)__popc(m), &got);
+                    stop = *(volatile ull *)&a.status->err != 0ull;
+                }
+                base = __shfl_sync(FULL, base, 0);
+            } else {
+                uint32_t b32 = 0;                  // the batch queue's counter is 32-bit
+                if (lane == 0) {
+                    if (m) b32 = atomicAdd(&a.status->ext_next, (uint32_t)__popc(m));
+                    stop = *(volatile ull *)&a.status->err != 0ull;
+                }
+                base = __shfl_sync(FULL, b32, 0);
             }
-            base = __shfl_sync(FULL, base, 0);
             stop = __shfl_sync(FULL, stop, 0);
             if (stop) break;                                             // warp-uniform
-            if ((uint64_t)base + __popc(m) >= njobs) drained = true;     // warp-uniform
+            if (RING) {
+                got = __shfl_sync(FULL, got, 0);
+                if (got < (uint32_t)__popc(m)) drained = true;           // the ring is empty for now
+            } else if (base + __popc(m) >= njobs) {
+                drained = true;                                          // warp-uniform
+            }
             if (need) {
-                const uint64_t jidx = (uint64_t)base + __popc(m & ((1u << lane) - 1u));
-                if (jidx < njobs) {
-                    myjob = (uint32_t)jidx;
+                const uint32_t rank = __popc(m & ((1u << lane) - 1u));
+                const uint64_t jidx = base + rank;
+                bool have = RING ? rank < got : jidx < njobs;
+                if (RING && have) {
+                    have = ring_wait_ready(a, jidx);
+                    mypos = jidx;
+                }
+                if (have) {
+                    myjob = (uint32_t)(RING ? (jidx & a.ring_mask) : jidx);
                     old = false;
+                    took = true;
                     // ---- phase A: one 4-set per lane
-                    pending = job_setup(a, jidx, J, w->fp, lane);
+                    pending = job_setup<RING>(a, myjob, J, w->fp, lane);
                     const bool big = pending && J.L + J.H > (uint32_t)DCAP;
                     if (pending) {
                         cnt.use(a, J.item);
@@ -608,6 +782,7 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                         extend_big(a, J, myjob, cnt.cand, cnt.sqrt_, w->ext, &w->n_ext);
                         pending = false;
                     }
+                    if (RING && !pending) rel = true;                  // done in phase A: freed after the report
                 }
             }
         }
@@ -769,19 +944,134 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
                 cnt.use(a, J.item);
                 cnt.sqrt_ += w->jsq[lane];
                 w->jsq[lane] = 0;
+                if (RING) rel = true;
             }
             pending = pending && !fits;
             old = pending;
         }
         __syncwarp();
         if (lane == 0 && w->n_ext) {          // this round's extensions (and any from the per-lane path)
-            report_warp_exts(a, w->ext, min(w->n_ext, (uint32_t)EXCAP));
+            report_warp_exts<RING>(a, w->ext, min(w->n_ext, (uint32_t)EXCAP));
             w->n_ext = 0;
         }
         __syncwarp();
+        if (RING) {                            // the round's finished 4-sets hand their slots back
+            const unsigned rm = __ballot_sync(FULL, rel);
+            if (rel) ring_release(a, mypos);
+            rel = false;
+            if (lane == 0 && rm) atomicAdd(&a.status->q_freed, (ull)__popc(rm));
+        }
         if (!round && drained) break;          // warp-uniform
     }
     cnt.flush(a);
+    return RING ? __any_sync(FULL, took) : false;
+}
+
+__global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
+    extern __shared__ __align__(16) unsigned char esmem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    WarpArea *w = (WarpArea *)(esmem + (size_t)wid * sizeof(WarpArea));
+    const uint64_t njobs = min(*(volatile ull *)&a.status->n_jobs, (ull)a.jobs_cap);
+    engine_loop<false>(a, w, lane, njobs);
+}
+
+// ================================================================== the persistent kernel
+
+// One launch for a whole call.  Every CTA (PBS threads, three per SM) loops over two roles:
+// producing -- claim the next group of SUPER_K tiles of 2^13 S (highest cost first), run P1-P5
+// and write the 4-sets into the ring -- or consuming -- its warps run the extension engine on
+// 4-sets claimed from the ring.  A CTA consumes while at least CONSUME_AT 4-sets are queued,
+// produces while tiles are left and the ring is less than half full, and ends when every tile is
+// produced and every 4-set claimed.  The roles switch with hysteresis: a CTA turns to the engine
+// when ring_high 4-sets are queued, and its warps keep claiming until fewer than ring_low are
+// left (while tiles remain), so that every warp has 4-sets to pool, claims take the add path,
+// and role changes are rare next to the work between them.  A call of any number of subranges is
+// one launch.  The tile layout and the engine's warp areas share the CTA's shared memory (one
+// role at a time).
+constexpr int PTL = 13;
+constexpr int PWARPS = PBS / 32;
+static_assert(TileLayout<PTL>::OFF_ELIST + SUPER_K * PWARPS * sizeof(uint32_t) <= PWARPS * sizeof(WarpArea),
+              "the tile layout fits in the engine's warp areas");
+static_assert(PWARPS * sizeof(WarpArea) + 1024 <= 228 * 1024 / 3, "three persistent CTAs per SM");
+
+__global__ void __launch_bounds__(PBS, 3) search_persist(const SearchArgs a) {
+    using L = TileLayout<PTL>;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ TileShared ts;
+    __shared__ unsigned long long s_base, s_idle0;
+    __shared__ unsigned int s_claim;
+    __shared__ int s_store, s_role, s_busy;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    uint64_t *lists = a.raw ? a.raw + (size_t)blockIdx.x * SUPER_K * a.raw_cap : nullptr;
+    uint32_t *raw_n = (uint32_t *)(smem + L::OFF_ELIST);
+    const uint32_t slice = a.raw ? a.raw_cap / PWARPS : 0;
+    if (tid == 0) s_idle0 = 0;
+    for (;;) {
+        if (tid == 0) {
+            int role = 2;                                    // 0 end, 1 produce, 2 consume
+            if (ld_vol(&a.status->err) != 0ull) {
+                role = 0;
+            } else {
+                const ull tail = ld_vol(&a.status->q_tail), head = ld_vol(&a.status->q_head);
+                const ull freed = ld_vol(&a.status->q_freed);
+                const uint32_t tn = ld_vol(&a.status->tile_next);
+                const long long queued = (long long)(tail - head);
+                if (queued >= (long long)a.ring_high || (tn >= a.n_tiles && queued > 0)) {
+                    role = 2;
+                } else if (tn < a.n_tiles && tail - freed < (a.jobs_cap >> 1)) {
+                    const uint32_t c = atomicAdd(&a.status->tile_next, SUPER_K);
+                    if (c < a.n_tiles) {
+                        role = 1;
+                        s_claim = c;
+                    }
+                } else if (tn >= a.n_tiles && ld_vol(&a.status->q_produced) >= a.n_tiles && queued <= 0) {
+                    role = 0;
+                }
+            }
+            s_role = role;
+            s_busy = 0;
+        }
+        __syncthreads();
+        const int role = s_role;
+        if (role == 0) break;                                // block-uniform
+        if (role == 1) {
+            const uint32_t cn = produce_group<PTL, PBS, true>(a, ts, smem, s_claim, lists, raw_n, slice, s_base, s_store);
+            if (tid == 0) {
+                __threadfence();
+                atomicAdd(&a.status->q_produced, (ull)cn);
+                s_idle0 = 0;
+            }
+        } else {
+            WarpArea *w = (WarpArea *)(smem + (size_t)wid * sizeof(WarpArea));
+            if (engine_loop<true>(a, w, lane, 0) && lane == 0) s_busy = 1;
+            __syncthreads();
+            if (tid == 0) {
+                if (s_busy) {
+                    s_idle0 = 0;
+                } else {                                     // nothing to take: wait a little, bounded
+                    const uint64_t t = gtimer();
+                    if (!s_idle0) s_idle0 = t;
+                    else if (t - s_idle0 > 2 * WAIT_NS) raise_error(a.status, E_TIMEOUT, 4);
+                    __nanosleep(1000);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// One consumer wait on position 0 of a one-slot ring that nothing publishes, with tiles still
+// unproduced: the wait must give up after WAIT_NS and record E_TIMEOUT (ps4_check_ring_wait).
+__global__ void ring_wait_probe(const SearchArgs a, unsigned long long *out) {
+    const uint64_t t0 = gtimer();
+    out[0] = ring_wait_ready(a, 0) ? 1ull : 0ull;
+    out[1] = gtimer() - t0;
+}
+
+// seq[i] = i: every slot free for its first lap
+__global__ void ring_init(uint32_t *seq, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        seq[i] = (uint32_t)i;
 }
 
 // ================================================================== launchers
@@ -805,6 +1095,25 @@ int launch_gen(const SearchArgs &a, int grid, void *stream) {
         case 13: return launch_gen_tl<13>(a, grid, s);
         default: return launch_gen_tl<14>(a, grid, s);
     }
+}
+
+int persist_ctas_per_sm() { return 3; }
+
+int launch_persist(const SearchArgs &a, int grid, void *stream) {
+    const size_t smem = PWARPS * sizeof(WarpArea);
+    cudaFuncSetAttribute(search_persist, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    search_persist<<<grid, PBS, smem, (cudaStream_t)stream>>>(a);
+    return (int)cudaGetLastError();
+}
+
+int launch_ring_wait_probe(const SearchArgs &a, unsigned long long *out, void *stream) {
+    ring_wait_probe<<<1, 1, 0, (cudaStream_t)stream>>>(a, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_ring_init(uint32_t *seq, uint64_t n, void *stream) {
+    ring_init<<<1184, 256, 0, (cudaStream_t)stream>>>(seq, n);
+    return (int)cudaGetLastError();
 }
 
 int launch_ext(const SearchArgs &a, int grid, void *stream) {

@@ -28,7 +28,8 @@ enum {
     E_VERIFY = PS4_ERR_VERIFY,
     E_TILE = 100,      // a tile outgrew its shared-memory lists: re-run with smaller tiles
     E_EXTLIST = 101,   // more extensions than a tile's (fused kernel) or an engine round's list holds
-    E_QUEUE = 102      // the 4-set job queue of a batch overflowed: re-run with narrower batches
+    E_QUEUE = 102,     // the 4-set job queue of a batch overflowed: re-run with narrower batches
+    E_TIMEOUT = PS4_ERR_TIMEOUT   // a bounded wait of the persistent kernel gave up (code | where << 8)
 };
 
 // One query segment: every S in [lo, hi) of query item `id`.  Tiles of the segment are
@@ -51,6 +52,11 @@ struct Status {
     unsigned long long n_jobs;     // 4-sets queued by gen_jobs
     unsigned int tile_next;        // tile work counter of the tile kernels (tiles handed out)
     unsigned int ext_next;         // extend_jobs work counter (queued 4-sets handed out)
+    // the persistent kernel's 4-set ring (positions count up from 0 over a call; slot = pos & mask)
+    unsigned long long q_tail;     // positions reserved by producing CTAs
+    unsigned long long q_head;     // positions claimed by consuming warps
+    unsigned long long q_freed;    // positions whose 4-set is finished and whose slot is free again
+    unsigned long long q_produced; // tiles whose 4-sets are all written
 };
 
 // Arguments of one search launch (passed by value).
@@ -75,8 +81,19 @@ struct SearchArgs {
     uint32_t *jobs;            // 4-set job queue between gen_jobs and extend_jobs: 6 * jobs_cap u32 (SoA)
     uint64_t jobs_cap;
     uint64_t *raw;             // optional (gen_jobs): per CTA, SUPER_K lists of one tile's representations,
-    uint32_t raw_cap;          //   raw_cap entries each, in NWARP equal warp slices
+    uint32_t raw_cap;          //   raw_cap entries each, in one equal slice per warp
+    // persistent kernel: jobs is a ring of jobs_cap (a power of two) slots; seq[slot] tells its state
+    // for position pos = slot + lap * jobs_cap: pos = free for pos, pos + 1 = 4-set of pos written
+    uint32_t *seq;
+    uint64_t ring_mask;        // jobs_cap - 1
+    uint64_t ring_fast;        // claims may take positions without a compare-and-swap while this many
+                               //   reserved positions are unclaimed (> every warp's claim at once)
+    uint64_t ring_high;        // a CTA turns to the engine when this many 4-sets are queued ...
+    uint64_t ring_low;         //   and its warps stop claiming below this many while tiles are left
 };
+// the persistent kernel's threads per CTA, and the time any of its waits may take before it gives up
+constexpr int PBS = 256;
+constexpr unsigned long long WAIT_NS = 2000000000ull;
 // representations a tile's list holds: (pi/8) * 2^14 = 6434 expected, 8192 with margin
 constexpr uint32_t RAW_PER_TILE = 8192;
 // tiles a tile-kernel CTA claims at once and scans as one range: the scan of a tile costs
@@ -129,6 +146,11 @@ int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream);
 // two-kernel pipeline (ps4_extend.cu): 4-set generation into the job queue, then extension
 int launch_gen(const SearchArgs &a, int grid, void *stream);
 int launch_ext(const SearchArgs &a, int grid, void *stream);
+// the persistent kernel (ps4_extend.cu): tiles of 2^13 S, ring of a.jobs_cap slots
+int launch_persist(const SearchArgs &a, int grid, void *stream);
+int launch_ring_init(uint32_t *seq, uint64_t n, void *stream);
+int launch_ring_wait_probe(const SearchArgs &a, unsigned long long *out, void *stream);
+int persist_ctas_per_sm();
 int gen_grid(int num_sms);
 int ext_grid(int num_sms);
 int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);

@@ -37,6 +37,7 @@ PS4_F_DUMP4 = 4
 PS4_KERNEL_BATCHED = 0
 PS4_KERNEL_PLAIN = 1
 PS4_KERNEL_FUSED = 2
+PS4_KERNEL_PERSIST = 3
 
 PS4_GRAPH_AUTO = 0
 PS4_GRAPH_ALWAYS = 1
@@ -143,6 +144,7 @@ def load() -> C.CDLL:
         "ps4_search_range_noalloc": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64, P(Stats), P(Results)]),
         "ps4_search_enqueue": (C.c_int, [C.c_void_p, C.c_uint64, C.c_uint64]),
         "ps4_plan_shards": (C.c_int, [C.c_uint64, C.c_uint64, C.c_uint32, P(C.c_uint64)]),
+        "ps4_check_ring_wait": (C.c_int, [C.c_int, P(C.c_uint64)]),
         "ps4_check_roots": (C.c_int, [C.c_int, P(C.c_uint64), P(C.c_uint64), C.c_uint32, P(C.c_uint64),
                                       P(C.c_uint32)]),
         "ps4_search_finish": (C.c_int, [C.c_void_p, P(Stats), P(Results)]),

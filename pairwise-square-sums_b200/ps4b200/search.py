@@ -53,7 +53,7 @@ class Search:
         cfg.flags = ((_abi.PS4_F_NOEXT if noext else 0) | (_abi.PS4_F_VERIFY if verify else 0)
                      | (_abi.PS4_F_DUMP4 if dump4 else 0))
         cfg.kernel = {"batched": _abi.PS4_KERNEL_BATCHED, "plain": _abi.PS4_KERNEL_PLAIN,
-                      "fused": _abi.PS4_KERNEL_FUSED}[kernel]
+                      "fused": _abi.PS4_KERNEL_FUSED, "persist": _abi.PS4_KERNEL_PERSIST}[kernel]
         cfg.log2_tile = log2_tile
         cfg.ctas_per_sm = ctas_per_sm
         cfg.stream = stream

@@ -141,3 +141,16 @@ def test_4096_uneven_subranges_union_vs_fused_kernel(config3):
     for i in range(4096):
         assert sorted(got.get(i, [])) == sorted(fgot.get(i, [])), i
         assert_stats_equal(stats[i], fstats[i], label=f"fused item {i}")
+
+
+def test_4096_uneven_subranges_persistent_kernel_one_launch(config3):
+    """The same 4096 items through PS4_KERNEL_PERSIST -- the whole call as one persistent launch
+    over a ring of 4-sets -- equal the two-kernel pipeline's item by item."""
+    _, los, his, stats, got = config3
+    with Search(max(his) + 1, kernel="persist") as p:
+        pstats, pr = p.batch(los, his)
+        assert p.last_launches == 2                       # ring initialisation + the persistent kernel
+    pgot = _by_item(pr)
+    for i in range(4096):
+        assert sorted(got.get(i, [])) == sorted(pgot.get(i, [])), i
+        assert_stats_equal(stats[i], pstats[i], label=f"persist item {i}")
