@@ -402,7 +402,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--kernel", choices=["batched", "plain", "fused"], default="batched")
+    ap.add_argument("--kernel", choices=["batched", "plain", "fused", "persist"], default="batched")
     ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of s4 work per reference step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")

@@ -35,6 +35,7 @@ struct ps4_ctx {
     uint64_t tab_n = 0;
     uint64_t *d_spfq = nullptr;
     uint16_t *d_ndiv = nullptr;
+    uint4 *d_fac3 = nullptr;
     // working buffers (grown on demand)
     Item *d_items = nullptr; uint32_t items_cap = 0;
     unsigned long long *d_counters = nullptr; uint32_t counters_items = 0;
@@ -141,6 +142,7 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     cudaFree(c->d_spfq); cudaFree(c->d_ndiv); cudaFree(c->d_items); cudaFree(c->d_counters);
     cudaFree(c->d_hits); cudaFree(c->d_exts); cudaFree(c->d_sixes); cudaFree(c->d_quads);
     cudaFree(c->d_scratch); cudaFree(c->d_status); cudaFree(c->d_jobs); cudaFree(c->d_raw); cudaFree(c->d_seq);
+    cudaFree(c->d_fac3);
     cudaFree(c->d_tri_in); cudaFree(c->d_tri_state); cudaFree(c->d_tri_out); cudaFree(c->d_tri_cnt);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_segs) cudaFreeHost(c->h_segs);
@@ -195,6 +197,8 @@ extern "C" int ps4_create(const ps4_config *cfg, ps4_ctx **out) {
     CUDA_TRY(c, cudaMalloc((void **)&c->d_status, sizeof(Status)));
     CUDA_TRY(c, cudaMallocHost((void **)&c->h_status, sizeof(Status)));
     CUDA_TRY(c, (cudaError_t)launch_tables(c->d_spfq, c->d_ndiv, c->tab_n, c->stream));
+    CUDA_TRY(c, cudaMalloc((void **)&c->d_fac3, c->tab_n * sizeof(uint4)));
+    CUDA_TRY(c, (cudaError_t)launch_fac3(c->d_fac3, c->tab_n, c->stream));
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
     return PS4_OK;
 }
@@ -400,7 +404,7 @@ static int enqueue_items(ps4_ctx *c) {
     SearchArgs a;
     memset(&a, 0, sizeof a);
     a.log2_tile = TL;
-    a.spfq = c->d_spfq; a.ndiv = c->d_ndiv; a.tab_n = c->tab_n;
+    a.spfq = c->d_spfq; a.ndiv = c->d_ndiv; a.tab_n = c->tab_n; a.fac3 = c->d_fac3;
     a.counters = c->d_counters;
     a.hits = c->d_hits; a.hits_cap = c->hits_cap;
     a.exts = c->d_exts; a.exts_cap = c->exts_cap;
@@ -979,7 +983,7 @@ extern "C" int ps4_extend_triples(ps4_ctx *c, const uint64_t *abc, uint32_t n, u
 namespace ps4 {
 int ctx_view(ps4_ctx *c, CtxView *v) {
     if (!c || !c->d_spfq) return PS4_ERR_ARG;
-    v->spfq = c->d_spfq; v->ndiv = c->d_ndiv; v->tab_n = c->tab_n; v->s_hi_max = c->cfg.s_hi_max;
+    v->spfq = c->d_spfq; v->ndiv = c->d_ndiv; v->fac3 = c->d_fac3; v->tab_n = c->tab_n; v->s_hi_max = c->cfg.s_hi_max;
     v->cap_reps = c->cfg.cap_reps; v->cap_divs = c->cfg.cap_divs; v->cap_ext = c->cfg.cap_ext;
     v->flags = c->cfg.flags; v->device = c->cfg.device; v->num_sms = c->num_sms; v->stream = c->stream;
     return PS4_OK;

@@ -570,13 +570,15 @@ struct LaneJob {
 };
 
 // Factor D = m1*m2 (m1 = ra-rb, m2 = ra+rb, both < 2^23, of equal parity).  The power of two
-// comes from counting trailing zeros; the odd parts' walks (one table load per distinct prime)
-// run interleaved so that their dependent loads overlap.  m1's primes are stored from slot 0,
-// m2's from slot 8 (each has at most 7 distinct odd primes), then m2's are merged into m1's
-// list -- primes in first-seen order, as s4.c:141-147.  A new prime is written to a slot below
-// every unread slot of m2, so the merge is in place.
-__device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, uint32_t m2, uint32_t (*fp)[32],
-                                           int lane) {
+// comes from counting trailing zeros; each odd part's first three primes come in one 16-byte
+// load (fac3), and the rare cofactor left over is walked through spfq (one table load per
+// distinct prime), both walks interleaved so that their dependent loads overlap.  Without fac3
+// (null) every prime is walked through spfq.  m1's primes are stored from slot 0, m2's from
+// slot 8 (each has at most 7 distinct odd primes), then m2's are merged into m1's list --
+// primes in first-seen order, as s4.c:141-147.  A new prime is written to a slot below every
+// unread slot of m2, so the merge is in place.
+__device__ __forceinline__ int factor_pair(const uint64_t *spfq, const uint4 *fac3, uint32_t m1, uint32_t m2,
+                                           uint32_t (*fp)[32], int lane) {
     int na = 0, nb = 0;
     if (m1 > 1 && !(m1 & 1)) {                      // both even
         const uint32_t z1 = (uint32_t)__ffs((int)m1) - 1, z2 = (uint32_t)__ffs((int)m2) - 1;
@@ -584,6 +586,18 @@ __device__ __forceinline__ int factor_pair(const uint64_t *spfq, uint32_t m1, ui
         na = 1;
         m1 >>= z1;
         m2 >>= z2;
+    }
+    if (fac3) {
+        const uint4 fa = m1 > 1 ? __ldg(&fac3[m1]) : make_uint4(0, 0, 0, 1);
+        const uint4 fb = m2 > 1 ? __ldg(&fac3[m2]) : make_uint4(0, 0, 0, 1);
+        if (fa.x) fp[na++][lane] = fa.x;
+        if (fa.y) fp[na++][lane] = fa.y;
+        if (fa.z) fp[na++][lane] = fa.z;
+        if (fb.x) fp[8 + nb++][lane] = fb.x;
+        if (fb.y) fp[8 + nb++][lane] = fb.y;
+        if (fb.z) fp[8 + nb++][lane] = fb.z;
+        m1 = fa.w;
+        m2 = fb.w;
     }
     uint64_t sa = m1 > 1 ? __ldg(&spfq[m1]) : 0, sb = m2 > 1 ? __ldg(&spfq[m2]) : 0;
     while (m1 > 1 || m2 > 1) {
@@ -626,7 +640,7 @@ __device__ __forceinline__ bool job_setup(const SearchArgs &a, uint64_t j, LaneJ
         if (t != J.bi && t != J.bj) { if (o1 < 0) o1 = t; else o2 = t; }
     J.C1 = pick4(J.v, o1);
     J.C2 = pick4(J.v, o2);
-    J.np = factor_pair(a.spfq, ra - rb, ra + rb, fp, lane);
+    J.np = factor_pair(a.spfq, a.fac3, ra - rb, ra + rb, fp, lane);
     // D even => both factors even => 2 is the first prime and 4 | D
     J.has2 = J.np > 0 && (fp[0][lane] & 0xFFFFFFu) == 2;
     J.E2 = J.has2 ? fp[0][lane] >> 24 : 0;

@@ -68,6 +68,7 @@ struct SearchArgs {
     const uint64_t *spfq;      // spf | quot << 32, m < tab_n
     const uint16_t *ndiv;      // divisor counts, m < tab_n
     uint64_t tab_n;
+    const uint4 *fac3;         // odd m: up to three odd primes (p | e << 24, ascending) and the cofactor
     unsigned long long *counters;   // [n_items][K_SLOTS]
     ps4_hit *hits;   uint32_t hits_cap;
     ps4_ext *exts;   uint32_t exts_cap;
@@ -133,6 +134,7 @@ void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std
 struct CtxView {
     const uint64_t *spfq;
     const uint16_t *ndiv;
+    const uint4 *fac3;
     uint64_t tab_n, s_hi_max;
     uint32_t cap_reps, cap_divs, cap_ext, flags;
     int device, num_sms;
@@ -143,6 +145,7 @@ int ctx_fail(ps4_ctx *c, int code, const char *msg);
 
 // Launchers (ps4_kernels.cu).  Return a cudaError_t value.
 int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream);
+int launch_fac3(uint4 *fac3, uint64_t tab_n, void *stream);
 // two-kernel pipeline (ps4_extend.cu): 4-set generation into the job queue, then extension
 int launch_gen(const SearchArgs &a, int grid, void *stream);
 int launch_ext(const SearchArgs &a, int grid, void *stream);

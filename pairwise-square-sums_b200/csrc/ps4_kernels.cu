@@ -355,6 +355,33 @@ int launch_search(const SearchArgs &a, int kernel, int grid, void *stream) {
     }
 }
 
+// For odd m (the engine looks up odd parts only): its first three odd primes in ascending order,
+// each as p | e << 24, zero where m has fewer, and the cofactor m / (their powers), 1 when none
+// is left -- so the engine's factor walk of a difference takes one load for most m and continues
+// through spfq from the cofactor otherwise.  The prime order is the smallest-prime walk's
+// (s4.c:141-147).  Trial division, one thread per m.
+__global__ void build_fac3(uint4 *fac3, uint64_t n) {
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < n; m += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t w[3] = {0, 0, 0}, k = 0, x = (uint32_t)m;
+        if (m >= 2) {
+            while (!(x & 1)) x >>= 1;
+            for (uint32_t d = 3; d * d <= x && k < 3; d += 2) {
+                if (x % d) continue;
+                uint32_t e = 0;
+                while (x % d == 0) { x /= d; e++; }
+                w[k++] = d | (e << 24);
+            }
+            if (x > 1 && k < 3) { w[k++] = x | (1u << 24); x = 1; }
+        }
+        fac3[m] = make_uint4(w[0], w[1], w[2], m >= 2 ? x : 1u);
+    }
+}
+
+int launch_fac3(uint4 *fac3, uint64_t tab_n, void *stream) {
+    build_fac3<<<1184, 256, 0, (cudaStream_t)stream>>>(fac3, tab_n);
+    return (int)cudaGetLastError();
+}
+
 int launch_tables(uint64_t *spfq, uint16_t *ndiv, uint64_t tab_n, void *stream) {
     build_tables<<<1184, 256, 0, (cudaStream_t)stream>>>(spfq, ndiv, tab_n);
     return (int)cudaGetLastError();

@@ -582,7 +582,7 @@ int launch_step(ps4_server *s, StepBuf &b) {
         SearchArgs a;
         memset(&a, 0, sizeof a);
         a.items = b.d_items; a.n_items = n_items; a.n_tiles = tiles; a.log2_tile = TL;
-        a.spfq = s->v.spfq; a.ndiv = s->v.ndiv; a.tab_n = s->v.tab_n;
+        a.spfq = s->v.spfq; a.ndiv = s->v.ndiv; a.fac3 = s->v.fac3; a.tab_n = s->v.tab_n;
         a.counters = b.d_counters;
         a.hits = b.d_hits; a.hits_cap = (uint32_t)b.hits_cap;
         a.exts = b.d_exts; a.exts_cap = (uint32_t)b.exts_cap;
