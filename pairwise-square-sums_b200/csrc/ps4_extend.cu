@@ -123,20 +123,22 @@ __device__ __forceinline__ void ring_release(const SearchArgs &a, uint64_t pos) 
     *(volatile uint32_t *)&a.seq[pos & a.ring_mask] = (uint32_t)(pos + a.ring_mask + 1);
 }
 
-// Claim up to n positions below q_tail (one lane of a warp).  While tiles are left, fewer than
-// ring_low queued 4-sets are left for later (the warp stops consuming, its CTA turns to tiles).
-// While at least ring_fast reserved positions are unclaimed, an add cannot overtake the
-// reservations (every warp of the grid claiming at once takes fewer), so it is used; closer to
-// q_tail a compare-and-swap claims only what is reserved.  *got receives the count, the first
+// Claim up to n positions below q_tail (one lane of a warp).  The thresholds count published
+// 4-sets (q_pub), so that claims rarely land on positions still being written.  While tiles are
+// left, fewer than ring_low published 4-sets are left for later (the warp stops consuming, its
+// CTA turns to tiles).  While at least ring_fast published positions are unclaimed, an add cannot
+// overtake the reservations (every warp of the grid claiming at once takes fewer), so it is
+// used; closer to q_tail a compare-and-swap claims only what is reserved.  *got receives the count, the first
 // position is returned.
 __device__ __forceinline__ uint64_t ring_claim(const SearchArgs &a, uint32_t n, uint32_t *got) {
     ull *head = &a.status->q_head;
     ull h = ld_vol(head);
     const ull t = ld_vol(&a.status->q_tail);
+    const long long pub = (long long)(ld_vol(&a.status->q_pub) - h);   // published and unclaimed (about)
     *got = 0;
     if ((long long)(t - h) <= 0) return 0;
-    if (t - h < a.ring_low && ld_vol(&a.status->tile_next) < a.n_tiles) return 0;
-    if (t - h >= a.ring_fast) {
+    if (pub < (long long)a.ring_low && ld_vol(&a.status->tile_next) < a.n_tiles) return 0;
+    if (pub >= (long long)a.ring_fast) {
         *got = n;
         return atomicAdd(head, (ull)n);
     }
@@ -330,6 +332,7 @@ __device__ uint32_t produce_group(const SearchArgs &a, TileShared &ts, unsigned 
                 }
             }
             __syncthreads();
+            if (RING && tid == 0 && s_store && tot[0]) atomicAdd(&a.status->q_pub, (ull)tot[0]);
             tile_flush_counters(a, ts, item);
             __syncthreads();
         }
@@ -1004,14 +1007,18 @@ __global__ void __launch_bounds__(EBS, 3) extend_jobs(const SearchArgs a) {
 // role at a time).
 constexpr int PTL = 13;
 constexpr int PWARPS = PBS / 32;
-static_assert(TileLayout<PTL>::OFF_ELIST + SUPER_K * PWARPS * sizeof(uint32_t) <= PWARPS * sizeof(WarpArea),
-              "the tile layout fits in the engine's warp areas");
-static_assert(PWARPS * sizeof(WarpArea) + 1024 <= 228 * 1024 / 3, "three persistent CTAs per SM");
+// the tile state of the producing role sits in the dynamic area too, after the tile layout and
+// the group's list counters, so that the kernel's static shared memory stays a few words and three
+// CTAs (each with the 1 KB the hardware reserves per block) fit in the SM's 228 KB
+constexpr size_t P_TS_OFF = (TileLayout<PTL>::OFF_ELIST + SUPER_K * PWARPS * sizeof(uint32_t) + 15) & ~(size_t)15;
+static_assert(P_TS_OFF + sizeof(TileShared) <= PWARPS * sizeof(WarpArea),
+              "the tile layout and tile state fit in the engine's warp areas");
+static_assert(PWARPS * sizeof(WarpArea) + 1024 + 128 <= 228 * 1024 / 3, "three persistent CTAs per SM");
 
 __global__ void __launch_bounds__(PBS, 3) search_persist(const SearchArgs a) {
     using L = TileLayout<PTL>;
     extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ TileShared ts;
+    TileShared &ts = *reinterpret_cast<TileShared *>(smem + P_TS_OFF);
     __shared__ unsigned long long s_base, s_idle0;
     __shared__ unsigned int s_claim;
     __shared__ int s_store, s_role, s_busy;
@@ -1027,10 +1034,10 @@ __global__ void __launch_bounds__(PBS, 3) search_persist(const SearchArgs a) {
                 role = 0;
             } else {
                 const ull tail = ld_vol(&a.status->q_tail), head = ld_vol(&a.status->q_head);
-                const ull freed = ld_vol(&a.status->q_freed);
+                const ull freed = ld_vol(&a.status->q_freed), pub = ld_vol(&a.status->q_pub);
                 const uint32_t tn = ld_vol(&a.status->tile_next);
                 const long long queued = (long long)(tail - head);
-                if (queued >= (long long)a.ring_high || (tn >= a.n_tiles && queued > 0)) {
+                if ((long long)(pub - head) >= (long long)a.ring_high || (tn >= a.n_tiles && queued > 0)) {
                     role = 2;
                 } else if (tn < a.n_tiles && tail - freed < (a.jobs_cap >> 1)) {
                     const uint32_t c = atomicAdd(&a.status->tile_next, SUPER_K);
@@ -1111,7 +1118,17 @@ int launch_gen(const SearchArgs &a, int grid, void *stream) {
     }
 }
 
-int persist_ctas_per_sm() { return 3; }
+// resident CTAs per SM of the persistent kernel (three by design; fewer if the device says so, so
+// that no CTA of the grid waits for another to exit)
+int persist_ctas_per_sm() {
+    int n = 0;
+    if (cudaFuncSetAttribute(search_persist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(PWARPS * sizeof(WarpArea))) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, search_persist, PBS, PWARPS * sizeof(WarpArea)) !=
+            cudaSuccess)
+        n = 1;
+    return n < 1 ? 1 : (n > 3 ? 3 : n);
+}
 
 int launch_persist(const SearchArgs &a, int grid, void *stream) {
     const size_t smem = PWARPS * sizeof(WarpArea);

@@ -57,6 +57,7 @@ struct Status {
     unsigned long long q_head;     // positions claimed by consuming warps
     unsigned long long q_freed;    // positions whose 4-set is finished and whose slot is free again
     unsigned long long q_produced; // tiles whose 4-sets are all written
+    unsigned long long q_pub;      // 4-sets written and published (any order): what claims may count on
 };
 
 // Arguments of one search launch (passed by value).
