@@ -300,11 +300,12 @@ def config3_cpu_sample(los, his, budget_s: float = 12.0, seed: int = 5):
                       f"slowest region thread's own timer per s4 run"}
 
 
-def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = True, kernel: str = "persist",
-                      compare: str | None = "batched") -> dict:
+def measure_subranges(local: int, stream, steps: int, warmup: int, cpu: bool = True, kernel: str = "batched",
+                      compare: str | None = "persist") -> dict:
     """The batched uneven-subrange workload: 4096 subranges (seed 20261203, widths log-uniform
-    in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call: on the persistent kernel, one
-    launch over a ring of 4-sets, or on the two-kernel pipeline, autotuned.  value: S/s from the
+    in [1e5, 1e9], offsets uniform in [1, 1e11]) in one call: on the two-kernel pipeline,
+    autotuned, its launches captured as one CUDA graph, or on the persistent kernel, one launch
+    over a ring of 4-sets.  value: S/s from the
     library's CUDA events around each call's launches; e2e: the same calls timed from the host
     (pinned inputs copied in, results copied out and formatted).  `compare`: the other kernel,
     one step, its rate and whether every item's counters and lines equal."""
