@@ -260,6 +260,7 @@ __device__ inline void extend_quad(const SearchArgs &a, const uint32_t r[6], con
             const u128 e = usq - A;
             if (e == v[0] || e == v[1] || e == v[2] || e == v[3]) continue;
             n_sqrt++;
+            // e + C < u^2 + S < 2^89 (u <= (D+1)/2 < 2^44): inside is_square_fast's n < 2^100
             if (!is_square_fast(e + C1) || !is_square_fast(e + C2)) continue;
             const uint32_t slot = atomicAdd(elist_n, 1u);
             if (slot < elist_cap) {

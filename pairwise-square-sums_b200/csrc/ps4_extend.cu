@@ -704,6 +704,8 @@ __device__ __forceinline__ void process_queue(const SearchArgs &a, WarpArea *w, 
         const uint32_t jl = w->qj[idx];
         const EJob &J = w->job[jl];
         const u128 e = (u128)u * u - J.A;
+        // is_square_fast needs n < 2^100: u = (f+g)/2 <= (D+1)/2 < 2^44 and C < S < 2^44, so
+        // e + C < u^2 + C < 2^89
         if (is_square_fast(e + J.C1) && is_square_fast(e + J.C2)) {
             const uint32_t c = w->qidx[idx], l = c & 0xFFFu, h = (c >> 12) & 0xFFFu, d2 = c >> 24;
             const uint64_t fo = w->dbuf[J.base + l] * w->dbuf[J.base + J.L + h];

@@ -124,6 +124,8 @@ __global__ void __launch_bounds__(TBS) extend_triples_kernel(const TriArgs t) {
                             const uint64_t e = u * u - A;             // 0 < e <= dmax
                             if (e != A && e != B && e != C) {
                                 nsqrt++;
+                                // e <= dmax <= 2^62 and C < 2^44: e + C < 2^63, inside
+                                // is_square_fast's n < 2^100
                                 if (is_square_fast((u128)(e + C))) {
                                     const unsigned long long slot = atomicAdd(t.n_out, 1ull);
                                     if (slot < t.out_cap) {
