@@ -259,18 +259,21 @@ class Search:
         buf = C.create_string_buffer(_LINE_CAP)
         if r.n_hits:
             # every hit's lines in one call (ps4_format_hits), grown once if the estimate is short
+            # (the text buffer is kept between calls and only the bytes written are copied out)
             cap = max(1 << 16, 160 * r.n_hits + 48 * r.n_exts)
             items = (C.c_uint32 * (r.n_hits + r.n_exts))()
             nl = C.c_uint64()
             for _ in range(2):
-                big = C.create_string_buffer(cap)
-                n = self.lib.ps4_format_hits(self._hits, r.n_hits, self._exts, big, cap, items, C.byref(nl))
+                if getattr(self, "_fmt_cap", 0) < cap:
+                    self._fmt_buf, self._fmt_cap = C.create_string_buffer(cap), cap
+                n = self.lib.ps4_format_hits(self._hits, r.n_hits, self._exts, self._fmt_buf, self._fmt_cap, items,
+                                             C.byref(nl))
                 if n >= 0:
                     break
                 if n == -1:
                     raise Ps4Error(_abi.PS4_ERR_ARG, "a hit formats to more than 8 KB")
                 cap = -n
-            out.lines.extend(big.raw[:n].decode().splitlines(keepends=True))
+            out.lines.extend(C.string_at(self._fmt_buf, n).decode().splitlines(keepends=True))
             out.items.extend(items[:nl.value])
         for s in range(r.n_sixes):
             six = self._sixes[s]
