@@ -520,11 +520,12 @@ def main():
     (dev_s, e2e_s, kern_s), (S_all, cand_all) = aggregate(dist, world, [dev_s, e2e_s, kern_s],
                                                           [S_rank, cand_rank], "cuda")
 
-    plain = None
-    if world == 1 and args.kernel == "batched" and not args.no_plain:
-        with Search(hi, device=local, kernel="plain", stream=stream.cuda_stream) as sp:
-            sp.enqueue(lo, hi)
-            sp.finish(want_lines=False)
+    def other_kernel(kernel: str, warm: bool) -> dict:
+        """One timed step of [lo, hi) on another kernel choice, results checked against ours."""
+        with Search(hi, device=local, kernel=kernel, stream=stream.cuda_stream) as sp:
+            if warm:
+                sp.enqueue(lo, hi)
+                sp.finish(want_lines=False)
             flush.zero_()
             pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             pe0.record(stream)
@@ -532,10 +533,15 @@ def main():
             pe1.record(stream)
             pr = sp.finish(want_lines=False)
             torch.cuda.synchronize()
-            assert pr.stats == stats, "plain and batched kernels disagree"
+            assert pr.stats == stats, f"{kernel} and batched kernels disagree"
             pt = pe0.elapsed_time(pe1) / 1000.0
-            plain = {"value": (hi - lo) / pt, "unit": UNIT, "ms_per_step": 1000 * pt,
-                     "batched_over_plain": ((hi - lo) / (dev_s / args.steps)) / ((hi - lo) / pt)}
+        return {"value": (hi - lo) / pt, "unit": UNIT, "ms_per_step": 1000 * pt,
+                "batched_over_" + kernel: ((hi - lo) / (dev_s / args.steps)) / ((hi - lo) / pt)}
+
+    plain = fused = None
+    if world == 1 and args.kernel == "batched" and not args.no_plain:
+        plain = other_kernel("plain", warm=False)       # one thread per S: 28 s, no warm-up needed
+        fused = other_kernel("fused", warm=True)        # tiles, staging and per-lane extension in one kernel
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -604,6 +610,7 @@ def main():
         "gpu_launches": launches,
         "clocks": clk,
         "plain_gpu": plain,
+        "fused_gpu": fused,
         "cpu_baseline": cpu,
         "triples": triples,
         "subranges": subranges,
