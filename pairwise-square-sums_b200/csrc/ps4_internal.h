@@ -102,8 +102,9 @@ constexpr uint32_t RAW_PER_TILE = 8192;
 // ~0.29 sqrt(S) steps whatever its width, so one scan of SUPER_K adjacent tiles, recorded into
 // their lists, divides that cost by SUPER_K (lists: 296 CTAs x 8 x 64 KB = 155 MB)
 constexpr uint32_t SUPER_K = 8;
-// below this S a tile's own scan is cheaper than recording and reading the lists
-constexpr uint64_t SUPER_MIN_S = 10000000000ull;
+// below this S a tile's own scan is cheaper than recording and reading the lists (per [1,1e10)
+// step of the tile kernel: from 5e9 224.2 -> 219.3 ms; from 2e9 222.6; from 1e9 224.4)
+constexpr uint64_t SUPER_MIN_S = 5000000000ull;
 
 // Arguments of one triple-extension launch (ps4_triples.cu).
 struct TriArgs {
