@@ -333,7 +333,8 @@ void ps4_serve_get_info(const ps4_server *srv, ps4_serve_info *info);
  * fixed compile-time sizes, s4.c:46-52). */
 typedef struct {
     uint32_t log2_tile;       /* 12 .. 14                                                            */
-    uint32_t gen_ctas;        /* 1 .. 2                                                              */
+    uint32_t gen_ctas;        /* 1 .. 2: tile-kernel threads per SM in units of 512 (512-thread CTAs  */
+                              /* on 2^14-S tiles, 256-thread ones on smaller tiles)                 */
     uint32_t ext_ctas;        /* 1 .. 3                                                              */
     uint32_t log2_jobs;       /* 20 .. 29                                                            */
     double rate;              /* S/s the tuner measured for this shape (0 if set by hand)            */

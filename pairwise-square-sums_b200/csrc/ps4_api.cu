@@ -49,7 +49,7 @@ struct ps4_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double last_ms = 0.0;
     uint64_t last_launches = 0;
-    unsigned tile_log2 = 14;             // current tile size (may shrink on E_TILE)
+    unsigned tile_log2 = 13;             // current tile size (may shrink on E_TILE)
     PendingSearch pend;
     uint64_t *d_raw = nullptr;           // per tile-kernel CTA: SUPER_K tile lists of RAW_PER_TILE
     uint64_t raw_words = 0;
@@ -65,7 +65,7 @@ struct ps4_ctx {
     uint64_t ring_cap = 1ull << 26;
     uint64_t h2d_bytes = 0, d2h_bytes = 0;
     // tuning (ps4_autotune / ps4_set_tuning)
-    uint32_t gen_ctas = 2, ext_ctas = 3;     // resident CTAs per SM of the tile kernel / the engine
+    uint32_t gen_ctas = 2, ext_ctas = 3;     // per SM: tile-kernel threads in units of 512 / engine CTAs
     uint64_t jobs_cap_max = 1ull << 29;      // largest job queue (entries; 2^29 = 12.9 GB): fewer,
                                              //   longer batches, fewer launch tails
     double tuned_rate = 0.0;
@@ -171,6 +171,9 @@ extern "C" int ps4_create(const ps4_config *cfg, ps4_ctx **out) {
         *out = c;
         return rc;
     }
+    // default tiles: 2^13 S for the two-kernel pipeline (four 256-thread tile CTAs per SM), 2^14
+    // for the one-kernel designs, whose CTAs keep 512 threads
+    if (c->cfg.kernel != PS4_KERNEL_BATCHED) c->tile_log2 = 14;
     if (c->cfg.log2_tile) c->tile_log2 = std::min(14u, std::max(12u, c->cfg.log2_tile));
     *out = c;
     int ndev = 0;
@@ -415,7 +418,7 @@ static int enqueue_items(ps4_ctx *c) {
     a.flags = c->cfg.flags & (p.dump ? ~0u : ~(uint32_t)PS4_F_DUMP4);
     a.jobs = c->d_jobs;
     a.jobs_cap = c->jobs_cap;
-    if (kernel == PS4_KERNEL_BATCHED) { a.raw = c->d_raw; a.raw_cap = RAW_PER_TILE; }
+    if (kernel == PS4_KERNEL_BATCHED) { a.raw = c->d_raw; a.raw_cap = raw_cap_for(TL); }
     if (persist) {
         a.jobs_cap = c->ring_cap;
         a.seq = c->d_seq;
@@ -427,7 +430,9 @@ static int enqueue_items(ps4_ctx *c) {
         a.raw_cap = raw_cap_persist;
     }
     const bool ext = !(c->cfg.flags & PS4_F_NOEXT);
-    const int g_gen = c->num_sms * (int)c->gen_ctas, g_ext = c->num_sms * (int)c->ext_ctas;
+    // gen_ctas counts 512 threads per SM: one or two 512-thread CTAs on 2^14-S tiles, twice as
+    // many 256-thread ones on smaller tiles
+    const int g_gen = c->num_sms * (int)c->gen_ctas * (gen_threads(14) / gen_threads(TL)), g_ext = c->num_sms * (int)c->ext_ctas;
 
     // A call of several batches runs as one CUDA graph holding its whole launch sequence; the
     // graph is kept and replayed while the next call is the same (items, sizes, buffers).

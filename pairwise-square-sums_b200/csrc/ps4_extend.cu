@@ -1,6 +1,6 @@
 // ps4_extend.cu -- the batched search as two persistent kernels per batch of S:
 //
-//   gen_jobs<TL>  tiles of 2^TL S in shared memory (phases P1-P4 of ps4_device.cuh), then every
+//   gen_jobs<TL,NT>  tiles of 2^TL S in shared memory (P1-P4 of ps4_device.cuh), then every
 //                 4-set of the tile (P5: closed-form z ranges per representation pair) is
 //                 written to a global job queue: a count pass, one block scan, one atomic
 //                 reservation per tile, a write pass.                         (s4.c:280-341)
@@ -232,8 +232,8 @@ __device__ __forceinline__ uint32_t lane_pairs(const SearchArgs &a, uint32_t gw,
 }
 
 // One claimed group of tiles, the last-but-c0 SUPER_K tiles of the launch (tiles are taken from
-// the last one down, costliest first): per segment of the group one scan for all its tiles (from
-// S = SUPER_MIN_S up), then per tile P1-P4, the count pass, one reservation for the tile's
+// the last one down, costliest first): per segment of the group one scan for all its tiles (when
+// `lists` is given), then per tile P1-P4, the count pass, one reservation for the tile's
 // 4-sets, the write pass.  NT threads.  RING: the 4-sets go to the persistent kernel's ring and
 // each lane publishes its contiguous run after a fence.  Returns the number of tiles.
 template <int TL, int NT, bool RING>
@@ -262,7 +262,7 @@ __device__ uint32_t produce_group(const SearchArgs &a, TileShared &ts, unsigned 
         const uint64_t SA = it.lo + ((ti - it.tile_base) << TL);
         const uint64_t SB = min(it.hi, SA + ((uint64_t)ng << TL));
         const uint32_t item = it.id;
-        const bool grouped = lists != nullptr && SA >= SUPER_MIN_S;
+        const bool grouped = lists != nullptr;
         if (grouped) {
             if (tid < SUPER_K * NW) raw_n[tid] = 0;
             __syncthreads();
@@ -341,8 +341,8 @@ __device__ uint32_t produce_group(const SearchArgs &a, TileShared &ts, unsigned 
     return (uint32_t)cn;
 }
 
-template <int TL>
-__global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
+template <int TL, int NT>
+__global__ void __launch_bounds__(NT, BS / NT * 2) gen_jobs(const SearchArgs a) {
     using L = TileLayout<TL>;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ TileShared ts;
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
     // per tile of a group and warp: representations appended to the tile's list; in the tile
     // layout's extension-list area, which this kernel does not use otherwise
     uint32_t *raw_n = (uint32_t *)(smem + L::OFF_ELIST);
-    const uint32_t slice = a.raw ? a.raw_cap / NWARP : 0;
+    const uint32_t slice = a.raw ? a.raw_cap / (NT / 32) : 0;
     for (;;) {
         // claim SUPER_K tiles; tiles are taken from the last one down (costliest first)
         if (tid == 0) {
@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(BS, 2) gen_jobs(const SearchArgs a) {
         const bool stop = c0 >= a.n_tiles || ts.skip;
         __syncthreads();                                                 // s_claim read by all
         if (stop) break;                                                 // block-uniform
-        produce_group<TL, BS, false>(a, ts, smem, c0, lists, raw_n, slice, s_base, s_store);
+        produce_group<TL, NT, false>(a, ts, smem, c0, lists, raw_n, slice, s_base, s_store);
     }
 }
 
@@ -1099,15 +1099,16 @@ __global__ void ring_init(uint32_t *seq, uint64_t n) {
 
 // ================================================================== launchers
 
-int gen_grid(int num_sms) { return 2 * num_sms; }     // two 100 KB tile CTAs per SM
+int gen_grid(int num_sms, unsigned TL) { return num_sms * (BS / gen_threads(TL)) * 2; }
 int ext_grid(int num_sms) { return num_sms * 3; }
 
 template <int TL>
 static int launch_gen_tl(const SearchArgs &a, int grid, cudaStream_t s) {
     // the tile layout up to its extension-list area, then the group's list counters there
-    const size_t smem = TileLayout<TL>::OFF_ELIST + SUPER_K * NWARP * sizeof(uint32_t);
-    cudaFuncSetAttribute(gen_jobs<TL>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    gen_jobs<TL><<<grid, BS, smem, s>>>(a);
+    constexpr int NT = gen_threads(TL);
+    const size_t smem = TileLayout<TL>::OFF_ELIST + SUPER_K * (NT / 32) * sizeof(uint32_t);
+    cudaFuncSetAttribute(gen_jobs<TL, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    gen_jobs<TL, NT><<<grid, NT, smem, s>>>(a);
     return (int)cudaGetLastError();
 }
 

@@ -96,15 +96,21 @@ struct SearchArgs {
 // the persistent kernel's threads per CTA, and the time any of its waits may take before it gives up
 constexpr int PBS = 256;
 constexpr unsigned long long WAIT_NS = 2000000000ull;
-// representations a tile's list holds: (pi/8) * 2^14 = 6434 expected, 8192 with margin
+// representations a 2^14-S tile's list holds: (pi/8) * 2^14 = 6434 expected, 8192 with margin;
+// a 2^TL-S tile's list holds raw_cap_for(TL), in proportion
 constexpr uint32_t RAW_PER_TILE = 8192;
+constexpr uint32_t raw_cap_for(unsigned TL) { return RAW_PER_TILE >> (14 - TL); }
 // tiles a tile-kernel CTA claims at once and scans as one range: the scan of a tile costs
 // ~0.29 sqrt(S) steps whatever its width, so one scan of SUPER_K adjacent tiles, recorded into
-// their lists, divides that cost by SUPER_K (lists: 296 CTAs x 8 x 64 KB = 155 MB)
-constexpr uint32_t SUPER_K = 8;
-// below this S a tile's own scan is cheaper than recording and reading the lists (per [1,1e10)
-// step of the tile kernel: from 5e9 224.2 -> 219.3 ms; from 2e9 222.6; from 1e9 224.4)
-constexpr uint64_t SUPER_MIN_S = 5000000000ull;
+// their lists, divides that cost by SUPER_K (lists: 592 CTAs x 16 x 32 KB = 310 MB; 16 tiles of
+// 2^13 S instead of 8: tile kernel -8 % at S = 5e11, per 5e8-S step).  With these tiles the group
+// scan pays at every S: per [1,1e10) step of the tile kernel 195.4 ms with groups from S = 5e9 up,
+// 161.0 from 1e9, 159.7 everywhere.
+constexpr uint32_t SUPER_K = 16;
+// threads of a tile-kernel CTA: 512 on 2^14-S tiles (two CTAs per SM), 256 on smaller ones (four
+// per SM).  At 2^13 S and four CTAs a barrier waits for 8 warps, not 16, and while one CTA waits
+// at it the other three issue: per [1,1e10) step of the tile kernel 219.2 -> 195.2 ms.
+constexpr int gen_threads(unsigned TL) { return TL >= 14 ? 512 : 256; }
 
 // Arguments of one triple-extension launch (ps4_triples.cu).
 struct TriArgs {
@@ -156,7 +162,7 @@ int launch_persist(const SearchArgs &a, int grid, void *stream);
 int launch_ring_init(uint32_t *seq, uint64_t n, void *stream);
 int launch_ring_wait_probe(const SearchArgs &a, unsigned long long *out, void *stream);
 int persist_ctas_per_sm();
-int gen_grid(int num_sms);
+int gen_grid(int num_sms, unsigned TL);      // the tile kernel's full residency for 2^TL-S tiles
 int ext_grid(int num_sms);
 int launch_search(const SearchArgs &a, int kernel, int grid, void *stream);
 int launch_triples(const TriArgs &t, void *stream);

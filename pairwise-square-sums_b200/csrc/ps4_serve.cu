@@ -225,7 +225,7 @@ enum { BUF_FREE = 0, BUF_KERNELS = 1, BUF_POST = 2 };
 struct StepBuf {
     int state = BUF_FREE;
     bool fused = false;
-    unsigned tile_log2 = 14;
+    unsigned tile_log2 = 13;
     std::vector<Chunk> chunks;
     std::vector<uint32_t> tris;           // triple queries of the step
     std::vector<uint32_t> queries;        // distinct queries of the step
@@ -283,7 +283,7 @@ struct ps4_server {
     std::vector<uint32_t> active;
     std::vector<int> free_slots;
     std::deque<uint32_t> unreported;
-    unsigned tile_log2 = 14;
+    unsigned tile_log2 = 13;
     uint32_t batch_div = 1;
     bool fused_next = false;
     uint64_t seq = 0;
@@ -592,8 +592,8 @@ int launch_step(ps4_server *s, StepBuf &b) {
         a.flags = s->v.flags & ~(uint32_t)PS4_F_DUMP4;
         a.jobs = s->d_jobs; a.jobs_cap = s->jobs_cap;
         if (!b.fused) {
-            a.raw = s->d_raw; a.raw_cap = RAW_PER_TILE;
-            const int g = (int)std::min<uint64_t>((uint64_t)gen_grid(s->v.num_sms), std::max<uint64_t>(tiles, 1));
+            a.raw = s->d_raw; a.raw_cap = raw_cap_for(TL);
+            const int g = (int)std::min<uint64_t>((uint64_t)gen_grid(s->v.num_sms, TL), std::max<uint64_t>(tiles, 1));
             SRV_CUDA(s, (cudaError_t)launch_gen(a, g, st));
             if (!(s->v.flags & PS4_F_NOEXT)) SRV_CUDA(s, (cudaError_t)launch_ext(a, ext_grid(s->v.num_sms), st));
         } else {
@@ -939,7 +939,8 @@ extern "C" int ps4_serve_create(ps4_ctx *ctx, const ps4_serve_config *cfg, ps4_s
     s->jobs_cap = 1ull << 20;
     while (s->jobs_cap < (1ull << 27) && (double)s->jobs_cap < need) s->jobs_cap <<= 1;
     if (dev_alloc(s, s->d_jobs, 6 * s->jobs_cap)) return PS4_ERR_CUDA;
-    if (dev_alloc(s, s->d_raw, (uint64_t)gen_grid(s->v.num_sms) * SUPER_K * RAW_PER_TILE)) return PS4_ERR_CUDA;
+    // lists for the tile kernel's full residency at any tile size (the same bytes at every size)
+    if (dev_alloc(s, s->d_raw, (uint64_t)gen_grid(s->v.num_sms, 14) * SUPER_K * RAW_PER_TILE)) return PS4_ERR_CUDA;
     if (dev_alloc(s, s->d_slots, c.max_slots)) return PS4_ERR_CUDA;
     for (int i = 0; i < 2; i++)
         if (init_buf(s, s->buf[i])) return PS4_ERR_CUDA;

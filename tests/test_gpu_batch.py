@@ -112,7 +112,7 @@ def test_4096_uneven_subranges_vs_single_calls_and_oracle(config3):
 @pytest.mark.skipif(not S4.exists(), reason="reference binary oracle/_ref/s4 not built")
 def test_4096_uneven_subranges_wide_high_items_vs_reference(config3):
     """Wide items (>= 1e8 S) at high offsets (>= 5e10), where the batch cutter splits an item
-    across batches and super-tiles scan, against the reference's own s4 on every host thread:
+    across batches, against the reference's own s4 on every host thread:
     sorted lines, all ten counters, the 5-set histogram and the CAPACITY maxima."""
     s, los, his, stats, got = config3
     threads = str(os.cpu_count() or 1)

@@ -9,7 +9,8 @@ device-side result buffers in one static array inside the library instead.
 Checked through the C-ABI against the regular entry point, ps4_search_range, on two calls in
 a row over different ranges (so the second call cannot pass on the first call's leftovers in
 the shared array), then on a repeat of the first range; then at S = 1e10 and 5e11, where the
-regular entry point scans super-tiles and this one does not; then the fixed
+tile scan costs most (the regular entry point scans groups of 16 tiles into lists, this one scans
+each of its own tiles); then the fixed
 result buffers overflowing.  The bar is bit-exact: counters and result lines equal.  The
 file is named to be collected last.
 """
@@ -75,7 +76,8 @@ def test_noalloc_matches_search_range_on_two_calls_in_a_row():
 
 @pytest.mark.parametrize("lo", [10 ** 10, 5 * 10 ** 11])
 def test_noalloc_matches_search_range_above_1e10(lo):
-    """From S = 5e9 up the regular entry point scans super-tiles; this one keeps its own tiles."""
+    """High S, where each tile's own scan (this entry point) and the regular entry point's scan of
+    16-tile groups into lists differ most in cost."""
     hi = lo + 10 ** 7
     with Search(hi) as s:
         want = s.range(lo, hi)
