@@ -18,20 +18,50 @@ static void put(sbuf *b, const char *s, size_t n) {
     if (b->bad || b->len + n + 1 > b->cap) { b->bad = 1; return; }
     memcpy(b->p + b->len, s, n);
     b->len += n;
-    b->p[b->len] = 0;
 }
-static void puts_(sbuf *b, const char *s) { put(b, s, strlen(s)); }
+#define PUTS(b, lit) put((b), (lit), sizeof(lit) - 1)
+
+/* decimal digits two at a time from a 200-byte pair table; 128-bit values are cut into
+ * 19-digit blocks first (one 128-bit division per block), so the digit loop runs on 64 bits */
+static const char DIG2[201] =
+    "00010203040506070809101112131415161718192021222324252627282930313233343536373839"
+    "40414243444546474849505152535455565758596061626364656667686970717273747576777879"
+    "8081828384858687888990919293949596979899";
+
+static int u64_digits(char *end, unsigned long long v) {  /* writes backwards from end, returns count */
+    char *p = end;
+    while (v >= 100) {
+        const unsigned r = (unsigned)(v % 100);
+        v /= 100;
+        p -= 2;
+        memcpy(p, DIG2 + 2 * r, 2);
+    }
+    if (v >= 10) { p -= 2; memcpy(p, DIG2 + 2 * v, 2); }
+    else *--p = (char)('0' + (int)v);
+    return (int)(end - p);
+}
+
+static void put_u64(sbuf *b, unsigned long long v) {
+    char tmp[24];
+    const int n = u64_digits(tmp + sizeof tmp, v);
+    put(b, tmp + sizeof tmp - n, (size_t)n);
+}
 
 static void put_u128(sbuf *b, u128 v) {
+    if ((v >> 64) == 0) { put_u64(b, (unsigned long long)v); return; }
+    const unsigned long long E19 = 10000000000000000000ull;
     char tmp[48];
-    int i = 0;
-    if (v == 0) { put(b, "0", 1); return; }
-    while (v) { tmp[i++] = (char)('0' + (int)(v % 10)); v /= 10; }
-    char out[48];
-    for (int j = 0; j < i; j++) out[j] = tmp[i - 1 - j];
-    put(b, out, (size_t)i);
+    char *end = tmp + sizeof tmp, *p = end;
+    while ((v >> 64) != 0) {                   /* low 19-digit blocks, zero-padded */
+        const unsigned long long blk = (unsigned long long)(v % E19);
+        v /= E19;
+        const int n = u64_digits(p, blk);
+        p -= n;
+        for (int k = n; k < 19; k++) *--p = '0';
+    }
+    p -= u64_digits(p, (unsigned long long)v);
+    put(b, p, (size_t)(end - p));
 }
-static void put_u64(sbuf *b, unsigned long long v) { put_u128(b, (u128)v); }
 
 static u128 ext_value(const ps4_ext *e) { return ((u128)e->hi << 64) | e->lo; }
 
@@ -40,33 +70,37 @@ static void put_set(sbuf *b, const char *tag, u128 *x, int n, uint64_t S, int ve
     for (int i = 0; i < n; i++)
         for (int j = i + 1; j < n; j++)
             if (x[j] > x[i]) { u128 t = x[i]; x[i] = x[j]; x[j] = t; }
-    puts_(b, tag);
-    puts_(b, " [");
+    put(b, tag, strlen(tag));
+    PUTS(b, " [");
     for (int i = 0; i < n; i++) {
         put_u128(b, x[i]);
         if (i < n - 1) put(b, ",", 1);
     }
-    puts_(b, "] S=");
+    PUTS(b, "] S=");
     put_u64(b, S);
-    if (!verified) puts_(b, "  *** VERIFY FAILED ***");
+    if (!verified) PUTS(b, "  *** VERIFY FAILED ***");
     put(b, "\n", 1);
 }
 
-static long done(sbuf *b) { return b->bad ? -1 : (long)b->len; }
+static long done(sbuf *b) {
+    if (b->bad) return -1;
+    b->p[b->len] = 0;                          /* put() keeps one byte free for it */
+    return (long)b->len;
+}
 
 long ps4_format_hit(const ps4_hit *h, const ps4_ext *exts, char *buf, size_t cap) {
     sbuf b = {buf, cap, 0, cap == 0};
     if (cap) buf[0] = 0;
     const ps4_ext *e = exts + h->first_ext;
     if (h->n_ext >= 2) {
-        puts_(&b, "M: [");
+        PUTS(&b, "M: [");
         for (int i = 0; i < 4; i++) { put_u64(&b, h->v[i]); if (i < 3) put(&b, ",", 1); }
-        puts_(&b, "] ext=[");
+        PUTS(&b, "] ext=[");
         for (uint32_t t = 0; t < h->n_ext; t++) {
             put_u128(&b, ext_value(&e[t]));
             if (t + 1 < h->n_ext) put(&b, ",", 1);
         }
-        puts_(&b, "] S=");
+        PUTS(&b, "] S=");
         put_u64(&b, h->S);
         put(&b, "\n", 1);
     }
@@ -96,11 +130,13 @@ long ps4_format_hits(const ps4_hit *hits, uint64_t n, const ps4_ext *exts, char 
             dst = tmp;
         }
         if (k < 0) return -1;                  /* a single hit longer than 8 KB: not produced by a search */
-        for (long c = 0; c < k; c++)
-            if (dst[c] == '\n') {
-                if (line_items && !full) line_items[lines] = hits[i].item;
-                lines++;
-            }
+        /* its lines: the M line (two or more extensions) and one 5: line per extension above max(v) */
+        const ps4_ext *e = exts + hits[i].first_ext;
+        uint32_t nh = hits[i].n_ext >= 2 ? 1u : 0u;
+        for (uint32_t t = 0; t < hits[i].n_ext; t++) nh += (e[t].flags & PS4_EXT_FIVE) ? 1u : 0u;
+        if (line_items && !full)
+            for (uint32_t j = 0; j < nh; j++) line_items[lines + j] = hits[i].item;
+        lines += nh;
         len += (size_t)k;
     }
     if (n_lines) *n_lines = lines;

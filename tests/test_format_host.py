@@ -56,3 +56,27 @@ def test_batch_formatter_matches_per_hit():
     assert n2 == -(n + 1) and nl.value == len(want_lines)
     got = small.value.decode()
     assert got == "".join(want_lines)[:len(got)] and got.endswith("\n") and len(got) < 1000
+
+
+def test_decimal_text_of_edge_values():
+    """Members, S and extensions print as Python's str(int) does: powers of ten, 2^64 -/+ 1,
+    128-bit values whose 19-digit blocks are zero or start with zeros, up to 2^128 - 1."""
+    lib = _abi.load()
+    edge = [1, 9, 10, 99, 100, 10 ** 18, 10 ** 19 - 1, 10 ** 19, 10 ** 19 + 1, 2 ** 64 - 1, 2 ** 64, 2 ** 64 + 1,
+            10 ** 20, 123 * 10 ** 19 + 5, 10 ** 38, 10 ** 38 - 1, 3 * 10 ** 38 + 7, 2 ** 127, 2 ** 128 - 1]
+    u64 = [x for x in edge if x < 2 ** 64]
+    buf = C.create_string_buffer(1 << 12)
+    for i, x in enumerate(edge):
+        h = _abi.Hit()
+        h.S = u64[i % len(u64)]
+        vs = [u64[(i + k) % len(u64)] for k in range(1, 5)]
+        for j in range(4):
+            h.v[j] = vs[j]
+        e = (_abi.Ext * 2)()
+        y = edge[(i + 7) % len(edge)]
+        for k, val in enumerate((x, y)):
+            e[k].lo, e[k].hi, e[k].flags = val & (2 ** 64 - 1), val >> 64, 0
+        h.n_ext, h.first_ext, h.flags = 2, 0, _abi.PS4_HIT_MULTI
+        n = lib.ps4_format_hit(C.byref(h), e, buf, len(buf))
+        want = f"M: [{','.join(map(str, vs))}] ext=[{x},{y}] S={h.S}\n"
+        assert n == len(want) and buf.value.decode() == want
