@@ -80,7 +80,7 @@ struct SearchArgs {
     Status *status;
     uint32_t cap_reps, cap_divs, cap_ext;
     uint32_t flags;            // PS4_F_*
-    uint32_t *jobs;            // 4-set job queue between gen_jobs and extend_jobs: 6 * jobs_cap u32 (SoA)
+    uint32_t *jobs;            // 4-set job queue between gen_jobs and extend_jobs: jobs_cap 24-byte records
     uint64_t jobs_cap;
     uint64_t *raw;             // optional (gen_jobs): per CTA, SUPER_K lists of one tile's representations,
     uint32_t raw_cap;          //   raw_cap entries each, in one equal slice per warp
