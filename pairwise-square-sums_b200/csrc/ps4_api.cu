@@ -53,7 +53,7 @@ struct ps4_ctx {
     PendingSearch pend;
     uint64_t *d_raw = nullptr;           // per tile-kernel CTA: SUPER_K tile lists of RAW_PER_TILE
     uint64_t raw_words = 0;
-    uint32_t *d_jobs = nullptr;          // 4-set job queue of the two-kernel pipeline (6 x jobs_cap u32)
+    uint32_t *d_jobs = nullptr;          // 4-set job queue of the two-kernel pipeline (jobs_cap 24-byte records)
     uint64_t jobs_cap = 1ull << 20;          // grows with the calls, up to jobs_cap_max
     uint64_t d_jobs_words = 0;
     uint32_t batch_div = 1;              // narrows the batches after a queue overflow
@@ -71,6 +71,11 @@ struct ps4_ctx {
     double tuned_rate = 0.0;
     // pinned staging of the segments, and the kept CUDA graph of a multi-batch call
     Item *h_segs = nullptr; uint64_t h_segs_cap = 0;
+    // pinned landing buffers of the result records (copied back at full speed, then ordered into the
+    // caller's buffers)
+    ps4_hit *h_hits = nullptr; uint64_t h_hits_cap = 0;
+    ps4_ext *h_exts = nullptr; uint64_t h_exts_cap = 0;
+    ps4_six *h_sixes = nullptr; uint64_t h_sixes_cap = 0;
     cudaGraphExec_t graph_exec = nullptr;
     std::string graph_key;
     uint64_t graph_launches = 0, graph_captures = 0, graph_replays = 0;
@@ -122,6 +127,19 @@ static int grow32(ps4_ctx *c, T *&ptr, uint32_t &cap, uint64_t need) {
     return rc;
 }
 
+// a pinned host buffer of at least `need` elements (grown by half again, kept between calls)
+template <class T>
+static int grow_pinned(ps4_ctx *c, T *&ptr, uint64_t &cap, uint64_t need) {
+    if (need <= cap && ptr) return 0;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    cap = 0;
+    const uint64_t n = std::max<uint64_t>(need + need / 2, 1024);
+    CUDA_TRY(c, cudaMallocHost((void **)&ptr, n * sizeof(T)));
+    cap = n;
+    return 0;
+}
+
 static uint64_t isqrt_host(uint64_t n) {
     uint64_t r = (uint64_t)std::sqrt((double)n);
     while (r * r > n) r--;
@@ -146,6 +164,9 @@ extern "C" void ps4_destroy(ps4_ctx *c) {
     cudaFree(c->d_tri_in); cudaFree(c->d_tri_state); cudaFree(c->d_tri_out); cudaFree(c->d_tri_cnt);
     if (c->h_status) cudaFreeHost(c->h_status);
     if (c->h_segs) cudaFreeHost(c->h_segs);
+    if (c->h_hits) cudaFreeHost(c->h_hits);
+    if (c->h_exts) cudaFreeHost(c->h_exts);
+    if (c->h_sixes) cudaFreeHost(c->h_sixes);
     if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
     for (cudaEvent_t e : c->kev) cudaEventDestroy(e);
     if (c->ev0) cudaEventDestroy(c->ev0);
@@ -235,35 +256,48 @@ double jobs_per_S_bound(uint64_t S_hi) {
 
 // Hits in a deterministic order -- item, S, then the reference's emission order (px, py, pz,
 // class) -- with each hit's extensions moved behind it and 6-set records re-pointed and sorted.
-void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std::vector<ps4_six> &sixes) {
-    std::vector<uint32_t> perm(hits.size());
-    for (uint32_t i = 0; i < perm.size(); i++) perm[i] = i;
-    std::sort(perm.begin(), perm.end(), [&](uint32_t x, uint32_t y) {
-        const ps4_hit &hp = hits[x], &hq = hits[y];
-        if (hp.item != hq.item) return hp.item < hq.item;
-        if (hp.S != hq.S) return hp.S < hq.S;
+// Writes the ordered hits and extensions to out_hits / out_exts (nh and the extensions' count
+// entries, not overlapping the inputs); sorts sixes in place.
+void canonical_order_into(const ps4_hit *hits, uint64_t nh, const ps4_ext *exts, ps4_six *sixes, uint64_t ns,
+                          ps4_hit *out_hits, ps4_ext *out_exts) {
+    struct Key {                       // the sort key next to the index: one contiguous array to sort
+        uint64_t S;
+        uint32_t item, o[4], idx;
+    };
+    std::vector<Key> key(nh);
+    for (uint64_t i = 0; i < nh; i++) {
+        const ps4_hit &h = hits[i];
+        key[i] = Key{h.S, h.item, {h.order[0], h.order[1], h.order[2], h.order[3]}, (uint32_t)i};
+    }
+    std::sort(key.begin(), key.end(), [](const Key &x, const Key &y) {
+        if (x.item != y.item) return x.item < y.item;
+        if (x.S != y.S) return x.S < y.S;
         for (int i = 0; i < 4; i++)
-            if (hp.order[i] != hq.order[i]) return hp.order[i] < hq.order[i];
+            if (x.o[i] != y.o[i]) return x.o[i] < y.o[i];
         return false;
     });
-    std::vector<ps4_hit> h2(hits.size());
-    std::vector<ps4_ext> e2;
-    e2.reserve(exts.size());
-    std::vector<uint32_t> newpos(hits.size());
-    for (uint32_t i = 0; i < perm.size(); i++) {
-        ps4_hit h = hits[perm[i]];
-        newpos[perm[i]] = i;
-        const uint32_t first = (uint32_t)e2.size();
-        for (uint32_t t = 0; t < h.n_ext; t++) e2.push_back(exts[h.first_ext + t]);
-        h.first_ext = first;
-        h2[i] = h;
+    std::vector<uint32_t> newpos(ns ? nh : 0);
+    uint32_t ne = 0;
+    for (uint64_t i = 0; i < nh; i++) {
+        ps4_hit h = hits[key[i].idx];
+        if (ns) newpos[key[i].idx] = (uint32_t)i;
+        if (h.n_ext) memcpy(out_exts + ne, exts + h.first_ext, h.n_ext * sizeof(ps4_ext));
+        h.first_ext = ne;
+        ne += h.n_ext;
+        out_hits[i] = h;
     }
-    for (auto &s6 : sixes) s6.hit = newpos[s6.hit];
-    std::sort(sixes.begin(), sixes.end(), [](const ps4_six &x, const ps4_six &y) {
+    for (uint64_t s = 0; s < ns; s++) sixes[s].hit = newpos[sixes[s].hit];
+    std::sort(sixes, sixes + ns, [](const ps4_six &x, const ps4_six &y) {
         if (x.hit != y.hit) return x.hit < y.hit;
         if (x.t != y.t) return x.t < y.t;
         return x.s < y.s;
     });
+}
+
+void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std::vector<ps4_six> &sixes) {
+    std::vector<ps4_hit> h2(hits.size());
+    std::vector<ps4_ext> e2(exts.size());
+    canonical_order_into(hits.data(), hits.size(), exts.data(), sixes.data(), sixes.size(), h2.data(), e2.data());
     hits.swap(h2);
     exts.swap(e2);
 }
@@ -664,39 +698,44 @@ static int finish_items(ps4_ctx *c, ps4_stats *stats, ps4_results *res) {
         std::vector<unsigned long long> k((size_t)n_items * K_SLOTS);
         CUDA_TRY(c, cudaMemcpyAsync(k.data(), c->d_counters, k.size() * sizeof(unsigned long long),
                                     cudaMemcpyDeviceToHost, c->stream));
-        std::vector<ps4_hit> hits(st.n_hits);
-        std::vector<ps4_ext> exts(st.n_exts);
-        std::vector<ps4_six> sixes(st.n_sixes);
-        if (st.n_hits)
-            CUDA_TRY(c, cudaMemcpyAsync(hits.data(), c->d_hits, st.n_hits * sizeof(ps4_hit), cudaMemcpyDeviceToHost,
-                                        c->stream));
-        if (st.n_exts)
-            CUDA_TRY(c, cudaMemcpyAsync(exts.data(), c->d_exts, st.n_exts * sizeof(ps4_ext), cudaMemcpyDeviceToHost,
-                                        c->stream));
-        if (st.n_sixes)
-            CUDA_TRY(c, cudaMemcpyAsync(sixes.data(), c->d_sixes, st.n_sixes * sizeof(ps4_six),
-                                        cudaMemcpyDeviceToHost, c->stream));
+        const bool fits = res && st.n_hits <= res->hits_cap && st.n_exts <= res->exts_cap &&
+                          st.n_sixes <= res->sixes_cap;
+        if (fits) {                              // the records land in pinned buffers, then go in order to res
+            if (grow_pinned(c, c->h_hits, c->h_hits_cap, st.n_hits) ||
+                grow_pinned(c, c->h_exts, c->h_exts_cap, st.n_exts) ||
+                grow_pinned(c, c->h_sixes, c->h_sixes_cap, st.n_sixes))
+                return PS4_ERR_CUDA;
+            if (st.n_hits)
+                CUDA_TRY(c, cudaMemcpyAsync(c->h_hits, c->d_hits, st.n_hits * sizeof(ps4_hit), cudaMemcpyDeviceToHost,
+                                            c->stream));
+            if (st.n_exts)
+                CUDA_TRY(c, cudaMemcpyAsync(c->h_exts, c->d_exts, st.n_exts * sizeof(ps4_ext), cudaMemcpyDeviceToHost,
+                                            c->stream));
+            if (st.n_sixes)
+                CUDA_TRY(c, cudaMemcpyAsync(c->h_sixes, c->d_sixes, st.n_sixes * sizeof(ps4_six),
+                                            cudaMemcpyDeviceToHost, c->stream));
+        }
         if (res && p.dump && st.n_quads)
             CUDA_TRY(c, cudaMemcpyAsync(res->quads, c->d_quads, st.n_quads * sizeof(ps4_quad), cudaMemcpyDeviceToHost,
                                         c->stream));
         CUDA_TRY(c, cudaStreamSynchronize(c->stream));
-        c->d2h_bytes += k.size() * sizeof(unsigned long long) + st.n_hits * sizeof(ps4_hit) +
-                        st.n_exts * sizeof(ps4_ext) + st.n_sixes * sizeof(ps4_six) +
+        c->d2h_bytes += k.size() * sizeof(unsigned long long) +
+                        (fits ? st.n_hits * sizeof(ps4_hit) + st.n_exts * sizeof(ps4_ext) +
+                                    st.n_sixes * sizeof(ps4_six)
+                              : 0) +
                         ((res && p.dump) ? st.n_quads * sizeof(ps4_quad) : 0);
         if (res) {
-            res->n_hits = hits.size();
-            res->n_exts = exts.size();
-            res->n_sixes = sixes.size();
-            if (res->n_hits > res->hits_cap || res->n_exts > res->exts_cap || res->n_sixes > res->sixes_cap) {
+            res->n_hits = st.n_hits;
+            res->n_exts = st.n_exts;
+            res->n_sixes = st.n_sixes;
+            if (!fits) {
                 p.active = true;                 // results stay on the device: finish may be called again
                 return set_err(c, PS4_ERR_OUTPUT_FULL, "result buffers too small: need hits=%llu exts=%llu sixes=%llu",
                                (unsigned long long)res->n_hits, (unsigned long long)res->n_exts,
                                (unsigned long long)res->n_sixes);
             }
-            canonical_order(hits, exts, sixes);
-            if (!hits.empty()) memcpy(res->hits, hits.data(), hits.size() * sizeof(ps4_hit));
-            if (!exts.empty()) memcpy(res->exts, exts.data(), exts.size() * sizeof(ps4_ext));
-            if (!sixes.empty()) memcpy(res->sixes, sixes.data(), sixes.size() * sizeof(ps4_six));
+            canonical_order_into(c->h_hits, st.n_hits, c->h_exts, c->h_sixes, st.n_sixes, res->hits, res->exts);
+            if (st.n_sixes) memcpy(res->sixes, c->h_sixes, st.n_sixes * sizeof(ps4_six));
         }
         if (stats)
             for (uint32_t i = 0; i < n_items; i++) stats_add(&stats[i], &k[(size_t)i * K_SLOTS]);

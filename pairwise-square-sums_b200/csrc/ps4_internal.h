@@ -137,6 +137,8 @@ void stats_add(ps4_stats *s, const unsigned long long *k);      // fold one coun
 const char *fatal_text(unsigned code);                            // the reference's FATAL message text
 double jobs_per_S_bound(uint64_t S_hi);                           // 4-set job queue entries per S, bound
 void canonical_order(std::vector<ps4_hit> &hits, std::vector<ps4_ext> &exts, std::vector<ps4_six> &sixes);
+void canonical_order_into(const ps4_hit *hits, uint64_t nh, const ps4_ext *exts, ps4_six *sixes, uint64_t ns,
+                          ps4_hit *out_hits, ps4_ext *out_exts);
 
 // Read-only view of a context (ps4_api.cu), for the allocation-free entry point and the server.
 struct CtxView {
