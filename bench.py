@@ -93,9 +93,14 @@ def _strata(width: int, lo: int, hi: int, k: int = 4):
             for j in range(k)]
 
 
-def cpu_sample_plan(lo: int, hi: int, budget_s: float):
+def cpu_sample_plan(lo: int, hi: int, budget_s: float, slice_w: int):
+    """The CPU sample: the reference's s4 on all host threads over 4 fixed slices of slice_w S (the
+    bench line's cpu_baseline and the reference arm time the same slices); the single-thread oracle
+    port, where s4 is not built, over slices sized to budget_s from a probe."""
     binary, kind = _s4_binary()
     threads = (os.cpu_count() or 1) if kind == "reference" else 1
+    if kind == "reference":
+        return binary, kind, threads, _strata(min(slice_w, max((hi - lo) // 8, 1)), lo, hi)
     w0 = 2 * 10 ** 7
     mid = (lo + hi) // 2
     t = _run_s4(binary, kind, mid, mid + w0, threads)
@@ -114,7 +119,7 @@ def run_reference(args, rank: int):
     if rank != 0:
         return
     lo, hi = 1, BOUND
-    binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=args.ref_budget)
+    binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=args.ref_budget, slice_w=args.ref_slice)
     for _ in range(args.warmup):
         cpu_sample_run(binary, kind, threads, slices)
     total_s, total_S = 0.0, 0
@@ -404,7 +409,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--kernel", choices=["batched", "plain", "fused", "persist"], default="batched")
-    ap.add_argument("--ref-budget", type=float, default=12.0, help="seconds of s4 work per reference step")
+    ap.add_argument("--ref-budget", type=float, default=12.0,
+                    help="seconds of work per reference step when only the single-thread oracle port is built")
+    ap.add_argument("--ref-slice", type=int, default=3 * 10 ** 8,
+                    help="S per slice of the reference's s4 (4 slices, the same in the reference arm and the "
+                         "bench line's cpu_baseline)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--workload", choices=["exhaustive", "subranges", "triples", "serve"], default="exhaustive",
@@ -545,7 +554,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=4.0)
+        binary, kind, threads, slices = cpu_sample_plan(lo, hi, budget_s=4.0, slice_w=args.ref_slice)
         secs, n = cpu_sample_run(binary, kind, threads, slices)
         cpu = {"value": n / secs, "unit": UNIT, "cores": threads, "kind": kind,
                "sample": f"{len(slices)} slices of {slices[0][1] - slices[0][0]} S at the midpoints of 4 equal "

@@ -19,8 +19,8 @@ PORT = REPO / "oracle" / "ps4_oracle"
 def _run(env_extra: dict) -> subprocess.CompletedProcess:
     env = dict(os.environ, **env_extra)
     return subprocess.run([sys.executable, str(REPO / "bench.py"), "--impl", "reference", "--steps", "1",
-                           "--warmup", "0", "--ref-budget", "0.4"], capture_output=True, text=True, env=env,
-                          timeout=600, cwd=REPO)
+                           "--warmup", "0", "--ref-budget", "0.4", "--ref-slice", "2000000"],
+                          capture_output=True, text=True, env=env, timeout=600, cwd=REPO)
 
 
 @pytest.mark.skipif(not S4.exists() and not PORT.exists(), reason="neither oracle/_ref/s4 nor the oracle port is built")
@@ -36,6 +36,8 @@ def test_reference_arm_line():
     cb = d["cpu_baseline"]
     assert cb["value"] == d["value"] and cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
     assert cb["kind"] == ("reference" if S4.exists() else "port")
+    if S4.exists():
+        assert "slices of 2000000 S" in cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
 
 
