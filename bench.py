@@ -611,7 +611,7 @@ def main():
                             f"{launches // max(args.steps, 1) // 2} batches)",
                      "ops": kernels[dom]["ops_per_step"], "traffic": kernels[dom]["traffic_per_step"],
                      "issue_active_ncu": kernels[dom]["issue_active_ncu"],
-                     "issue_active_source": f"profiles/ncu_{dom}_5e9.txt (1e8-S capture at S = 5e9)",
+                     "issue_active_source": f"profiles/ncu_{dom}_5e9.txt (5e8-S capture at S = 5e9)",
                      "step_achieved": achieved_step, "step_frac": achieved_step / peak,
                      "kernels": kernels},
         "e2e": {"value": S_all / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d // args.steps,
