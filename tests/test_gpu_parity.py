@@ -7,17 +7,21 @@ ranges are checked against the CPU restatement (oracle/) run on the same box.
 """
 from __future__ import annotations
 
+import os
 import random
+import subprocess
 
 import pytest
 
-from conftest import GOLDEN_DIR, assert_stats_equal, sha_sorted
+from conftest import GOLDEN_DIR, REPO, assert_stats_equal, sha_sorted
+from golden.make_golden import parse_stderr
 from oracle import orc
 from ps4b200 import Ps4Error, Search, _abi
 
 pytestmark = pytest.mark.gpu
 
 KERNELS = ("batched", "plain", "fused")
+S4 = REPO / "oracle" / "_ref" / "s4"
 
 
 @pytest.fixture(scope="module")
@@ -138,6 +142,22 @@ def test_frontier_blocks_wide():
             assert len(r.lines) == blk["n_lines"]
             assert sorted(x for x in r.lines if x.startswith("M:")) == blk["m_lines"], blk["block"]
             assert_stats_equal(r.stats, blk, hist=False, label=blk["block"])
+
+
+@pytest.mark.skipif(not S4.exists(), reason="reference binary oracle/_ref/s4 not built")
+@pytest.mark.parametrize("lo,width", [(12 * 10 ** 12, 2 * 10 ** 7), (17_500_000_000_000, 10 ** 7)])
+def test_top_of_range_vs_reference_s4(lo, width):
+    """At the reference's own frontier (S ~ 1.2e13) and just below the library's bound 2^44
+    (1.759e13), where roots approach 2^22 and the factor tables 8.4e6 entries: the reference's
+    s4 on every host thread over the same range -- sorted lines, all ten counters, the 5-set
+    histogram and the CAPACITY maxima."""
+    hi = lo + width
+    with Search(hi) as s:
+        r = s.range(lo, hi)
+    p = subprocess.run([str(S4), str(lo), str(hi), str(os.cpu_count() or 1), "20"], capture_output=True, text=True,
+                       check=True)
+    assert sorted(r.lines) == sorted(p.stdout.splitlines(keepends=True))
+    assert_stats_equal(r.stats, parse_stderr(p.stderr), label=f"s4 [{lo},{hi})")
 
 
 @pytest.mark.parametrize("seed", range(8))
