@@ -80,3 +80,25 @@ def test_decimal_text_of_edge_values():
         n = lib.ps4_format_hit(C.byref(h), e, buf, len(buf))
         want = f"M: [{','.join(map(str, vs))}] ext=[{x},{y}] S={h.S}\n"
         assert n == len(want) and buf.value.decode() == want
+
+
+def test_decimal_text_of_random_values():
+    """2,000 extensions of log-uniform bit length (1..128) and members and S of 1..64 bits print
+    as Python's str(int) does."""
+    lib = _abi.load()
+    rng = random.Random(2026)
+    buf = C.create_string_buffer(1 << 12)
+    for _ in range(1000):
+        h = _abi.Hit()
+        vs = [rng.getrandbits(rng.randint(1, 64)) or 1 for _ in range(4)]
+        for j in range(4):
+            h.v[j] = vs[j]
+        h.S = rng.getrandbits(rng.randint(1, 64))
+        xs = [rng.getrandbits(rng.randint(1, 128)) for _ in range(2)]
+        e = (_abi.Ext * 2)()
+        for k, val in enumerate(xs):
+            e[k].lo, e[k].hi, e[k].flags = val & (2 ** 64 - 1), val >> 64, 0
+        h.n_ext, h.first_ext, h.flags = 2, 0, _abi.PS4_HIT_MULTI
+        n = lib.ps4_format_hit(C.byref(h), e, buf, len(buf))
+        want = f"M: [{','.join(map(str, vs))}] ext=[{xs[0]},{xs[1]}] S={h.S}\n"
+        assert n == len(want) and buf.value.decode() == want
