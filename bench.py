@@ -18,8 +18,8 @@ e2e        the same through the public C-ABI call with host result buffers
 roofline   integer-issue roofline: algorithmic int32 lane-ops per launch (ps4b200/opmodel.py,
            frozen) / kernel time, against 4 warp-instructions x 32 lanes per SM per clock
 cpu_baseline  the reference's own s4 (oracle/_ref/s4, all host threads) on a stratified
-           sample of the same range, timed on this host
---impl reference  that CPU reference alone, as the reference arm
+           sample of the same range (4 slices of --ref-slice S), timed on this host
+--impl reference  that CPU reference alone over the same slices, as the reference arm
 """
 from __future__ import annotations
 
